@@ -1,0 +1,459 @@
+// C ABI of CuAPSS (include/cuapss.h) and the host orchestration of a join.
+//
+// The reference's orchestrator, similarity_join_device (fengyilin118/
+// APSS-CUDA similarity_search.cu:934-3014), copies 8 fixed partitions to the
+// device, builds per-partition indexes, then runs 28 cross-partition joins
+// and 8 self-joins, each through a dense n_A x n_B (or n(n-1)/2) float
+// accumulator in global memory with a blocking cudaThreadSynchronize after
+// every launch, and prints pair counts. Here one call handles a matrix of
+// any size: prepare (validate, remap, order, head block, inverted lists),
+// one persistent tile launch over the upper triangle of 128 x 128 pair
+// tiles with no n^2 buffer, then the exact finalize and a sorted pair list.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <string>
+
+#include "ctx.cuh"
+#include "index.cuh"
+#include "prep.cuh"
+#include "prims.cuh"
+#include "tiles.cuh"
+
+namespace cuapss {
+
+std::atomic<int64_t> g_launches{0};
+
+namespace {
+thread_local char g_last_error[512] = {0};
+}
+
+void record_cuda_error(cudaError_t e, const char* what, const char* file, int line) {
+  snprintf(g_last_error, sizeof(g_last_error), "%s: %s (%s:%d)", what, cudaGetErrorString(e),
+           file, line);
+}
+
+const char* last_error_message() { return g_last_error; }
+
+int choose_head_width(int precision, int64_t n, int64_t d, int64_t nnz) {
+  (void)n;
+  (void)nnz;
+  int p = precision == CUAPSS_PREC_MIXED ? 512 : 64;
+  const int64_t cap = ((d + 31) / 32) * 32;
+  if (p > cap) p = (int)cap;
+  return p;
+}
+
+cuapss_status stage_csr(cuapss_ctx* ctx, const cuapss_csr* x, const std::string& tag,
+                        DevCsr* out) {
+  if (!x || x->n < 0 || x->d < 1 || x->nnz < 0 || x->d > INT32_MAX || x->n >= INT32_MAX)
+    return CUAPSS_EINVAL;
+  if (!x->rowptr || (x->nnz > 0 && (!x->col || !x->val))) return CUAPSS_EINVAL;
+  out->n = x->n;
+  out->d = x->d;
+  out->nnz = x->nnz;
+  if (x->on_device) {
+    out->rp = x->rowptr;
+    out->col = x->col;
+    out->val = x->val;
+    return CUAPSS_OK;
+  }
+  int64_t* rp = nullptr;
+  int32_t* col = nullptr;
+  float* val = nullptr;
+  ST_TRY(ctx->ws.get(tag + ":in_rp", (size_t)x->n + 1, &rp));
+  ST_TRY(ctx->ws.get(tag + ":in_col", (size_t)std::max<int64_t>(x->nnz, 1), &col));
+  ST_TRY(ctx->ws.get(tag + ":in_val", (size_t)std::max<int64_t>(x->nnz, 1), &val));
+  cudaStream_t st = ctx->stream;
+  CU_TRY(cudaMemcpyAsync(rp, x->rowptr, sizeof(int64_t) * (x->n + 1), cudaMemcpyHostToDevice, st));
+  if (x->nnz > 0) {
+    CU_TRY(cudaMemcpyAsync(col, x->col, sizeof(int32_t) * x->nnz, cudaMemcpyHostToDevice, st));
+    CU_TRY(cudaMemcpyAsync(val, x->val, sizeof(float) * x->nnz, cudaMemcpyHostToDevice, st));
+  }
+  out->rp = rp;
+  out->col = col;
+  out->val = val;
+  return CUAPSS_OK;
+}
+
+namespace {
+
+float elapsed(cudaEvent_t a, cudaEvent_t b) {
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, a, b);
+  return ms;
+}
+
+}  // namespace
+
+cuapss_status join_device(cuapss_ctx* ctx, const DevCsr& a, const DevCsr* b, float t,
+                          cuapss_pairs* out, cuapss_stats* stats) {
+  const bool self = (b == nullptr);
+  const DevCsr& bb = self ? a : *b;
+  if (!self && a.d != bb.d) return CUAPSS_EINVAL;
+  if (!(t > 0.0f) || !std::isfinite(t)) return CUAPSS_EINVAL;
+  if (!out || out->capacity < 0) return CUAPSS_EINVAL;
+  if (out->capacity > 0 && (!out->i || !out->j || !out->sim)) return CUAPSS_EINVAL;
+  cudaStream_t st = ctx->stream;
+  Workspace& ws = ctx->ws;
+  const int64_t d = a.d;
+  const int64_t launches0 = g_launches.load();
+  cudaEventRecord(ctx->ev[0], st);
+  // ---- validate + posting counts + frequency remap ----
+  int32_t* counts = nullptr;
+  int32_t* perm = nullptr;
+  ST_TRY(ws.get("counts", (size_t)d, &counts));
+  ST_TRY(ws.get("perm", (size_t)d, &perm));
+  CU_TRY(cudaMemsetAsync(counts, 0, sizeof(int32_t) * d, st));
+  double nrm_a = 1.0, nrm_b = 1.0;
+  const int check = ctx->opts.validate;
+  ST_TRY(validate_csr(a.rp, a.col, a.val, a.n, d, a.nnz, ctx->opts.norm_tol, check, counts, &nrm_a,
+                      ws, "A", st));
+  if (!self)
+    ST_TRY(validate_csr(bb.rp, bb.col, bb.val, bb.n, d, bb.nnz, ctx->opts.norm_tol, check, counts,
+                        &nrm_b, ws, "B", st));
+  else
+    nrm_b = nrm_a;
+  ST_TRY(feature_perm(counts, d, a.n + (self ? 0 : bb.n), ctx->opts.remap, perm, ws, st));
+  const int precision = ctx->opts.precision;
+  int p = ctx->opts.head_width > 0 ? ctx->opts.head_width
+                                   : choose_head_width(precision, a.n + bb.n, d, a.nnz + bb.nnz);
+  p = (int)std::min<int64_t>(((int64_t)p + 31) / 32 * 32, ((d + 31) / 32) * 32);
+  PrepOptions po;
+  po.p = p;
+  po.want_head32 = 1;
+  Side SA, SB;
+  SA.rp0 = a.rp;
+  SA.col0 = a.col;
+  SA.val0 = a.val;
+  SA.n = a.n;
+  SA.d = d;
+  SA.nnz = a.nnz;
+  SA.nrm_max = nrm_a;
+  ST_TRY(build_side(SA, po, perm, ws, "A", st));
+  Side* SJ = &SA;
+  if (!self) {
+    SB.rp0 = bb.rp;
+    SB.col0 = bb.col;
+    SB.val0 = bb.val;
+    SB.n = bb.n;
+    SB.d = d;
+    SB.nnz = bb.nnz;
+    SB.nrm_max = nrm_b;
+    ST_TRY(build_side(SB, po, perm, ws, "B", st));
+    ST_TRY(link_tail(SA, SB, false, st));
+    SJ = &SB;
+  }
+  cudaEventRecord(ctx->ev[1], st);
+  // ---- pair tiles ----
+  const double u = std::ldexp(1.0, -24);
+  const double nrm2 = nrm_a * nrm_b;
+  TileArgs ta{};
+  ta.headI32 = SA.head32;
+  ta.nI = SA.n;
+  ta.nbI = SA.nb;
+  ta.tptrI = SA.tptr;
+  ta.tcur0 = SA.tcur0;
+  ta.tend = SA.tend;
+  ta.tr = SA.tr;
+  ta.tu = SA.tu;
+  ta.blkmaxI = SA.blk_maxnnz;
+  ta.hnormI = SA.hnorm;
+  ta.headJ32 = SJ->head32;
+  ta.nJ = SJ->n;
+  ta.nbJ = SJ->nb;
+  ta.cscJ = SJ->csc;
+  ta.blkmaxJ = SJ->blk_maxnnz;
+  ta.hnormJ = SJ->hnorm;
+  ta.p = SA.p;
+  ta.self = self ? 1 : 0;
+  ta.t = t;
+  ta.eps_c1 = u * nrm2 * 1.001;
+  ta.eps_c0 = 2.0 * u * nrm2 * 1.001 + 1e-10;
+  ta.eps_head = 0.0;
+  ta.nunits = self ? (int)((SA.nb + 1) / 2) : SA.nb;
+  int64_t ncand = 0;
+  int* unit_counter = nullptr;
+  int* err = nullptr;
+  unsigned long long* ccount = nullptr;
+  ST_TRY(ws.get("tiles:unit", 1, &unit_counter));
+  ST_TRY(ws.get("tiles:err", 1, &err));
+  ST_TRY(ws.get("tiles:ccount", 1, &ccount));
+  const int grid = std::max(1, std::min(ta.nunits, ctx->sms));
+  const int64_t stride = std::max<int64_t>(SA.max_block_tail, 1);
+  ST_TRY(ws.get("tiles:scr_cur", (size_t)grid * stride, &ta.scr_cur));
+  ST_TRY(ws.get("tiles:scr_next", (size_t)grid * stride, &ta.scr_next));
+  ta.scr_stride = stride;
+  ta.unit_counter = unit_counter;
+  ta.err = err;
+  ta.cand_count = ccount;
+  if (ctx->cand_cap == 0) ctx->cand_cap = std::max<int64_t>(1 << 20, 8 * (a.n + bb.n));
+  const int64_t ntiles = self ? (int64_t)SA.nb * (SA.nb + 1) / 2 : (int64_t)SA.nb * SJ->nb;
+  for (int attempt = 0; attempt < 3; ++attempt) {
+    ST_TRY(ws.get("cand:key", (size_t)ctx->cand_cap, &ta.cand_key));
+    ST_TRY(ws.get("cand:sim", (size_t)ctx->cand_cap, &ta.cand_sim));
+    ta.cand_cap = ctx->cand_cap;
+    CU_TRY(cudaMemsetAsync(unit_counter, 0, sizeof(int), st));
+    CU_TRY(cudaMemsetAsync(err, 0, sizeof(int), st));
+    CU_TRY(cudaMemsetAsync(ccount, 0, sizeof(unsigned long long), st));
+    if (ntiles > 0) ST_TRY(launch_tiles_fp32(ta, grid, st));
+    unsigned long long hc = 0;
+    int herr = 0;
+    CU_TRY(cudaMemcpyAsync(&hc, ccount, sizeof(hc), cudaMemcpyDeviceToHost, st));
+    CU_TRY(cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CU_TRY(cudaStreamSynchronize(st));
+    if (herr & kErrTimeout) return CUAPSS_ETIMEOUT;
+    if (herr) return CUAPSS_ECUDA;
+    ncand = (int64_t)hc;
+    if (ncand <= ctx->cand_cap) break;
+    ctx->cand_cap = ncand + ncand / 4;
+    if (attempt == 2) return CUAPSS_ENOMEM;
+  }
+  cudaEventRecord(ctx->ev[2], st);
+  // ---- finalize: exact decision, reported similarity, sorted output ----
+  uint64_t* okey = nullptr;
+  uint32_t* oidx = nullptr;
+  float* osim = nullptr;
+  unsigned long long* ocount = nullptr;
+  unsigned long long* nresc = nullptr;
+  const int64_t ocap = std::max<int64_t>(ncand, 1);
+  ST_TRY(ws.get("out:key", (size_t)ocap, &okey));
+  ST_TRY(ws.get("out:idx", (size_t)ocap, &oidx));
+  ST_TRY(ws.get("out:sim", (size_t)ocap, &osim));
+  ST_TRY(ws.get("out:count", 2, &ocount));
+  nresc = ocount + 1;
+  CU_TRY(cudaMemsetAsync(ocount, 0, 2 * sizeof(unsigned long long), st));
+  const int rbitsJ = std::max(1, bits_for((uint64_t)SJ->n));
+  const int rbitsI = std::max(1, bits_for((uint64_t)SA.n));
+  FinalizeArgs fa{};
+  fa.cand_key = ta.cand_key;
+  fa.cand_sim = ta.cand_sim;
+  fa.ncand = ncand;
+  fa.rowpermI = SA.rowperm;
+  fa.rowpermJ = SJ->rowperm;
+  fa.nnzI = SA.nnz_row;
+  fa.nnzJ = SJ->nnz_row;
+  fa.hnormI = SA.hnorm;
+  fa.hnormJ = SJ->hnorm;
+  fa.rpI = a.rp;
+  fa.colI = a.col;
+  fa.valI = a.val;
+  fa.rpJ = bb.rp;
+  fa.colJ = bb.col;
+  fa.valJ = bb.val;
+  fa.t = t;
+  fa.eps_c1 = ta.eps_c1;
+  fa.eps_c0 = ta.eps_c0;
+  fa.eps_head = ta.eps_head;
+  fa.self = self ? 1 : 0;
+  fa.rbits = rbitsJ;
+  fa.out_key = okey;
+  fa.out_idx = oidx;
+  fa.out_sim = osim;
+  fa.out_count = ocount;
+  fa.out_cap = ocap;
+  fa.n_rescored = nresc;
+  ST_TRY(launch_finalize(fa, st));
+  unsigned long long hcnt[2] = {0, 0};
+  CU_TRY(cudaMemcpyAsync(hcnt, ocount, sizeof(hcnt), cudaMemcpyDeviceToHost, st));
+  CU_TRY(cudaStreamSynchronize(st));
+  const int64_t npairs = (int64_t)hcnt[0];
+  ST_TRY(radix_sort_pairs(okey, oidx, npairs, rbitsI + rbitsJ, ws, "out", st));
+  out->count = npairs;
+  cuapss_status result = CUAPSS_OK;
+  if (npairs > out->capacity) {
+    result = CUAPSS_EOVERFLOW;
+  } else if (npairs > 0) {
+    if (out->on_device) {
+      ST_TRY(launch_split_pairs(okey, oidx, osim, npairs, rbitsJ, out->i, out->j, out->sim, st));
+    } else {
+      int32_t *di = nullptr, *dj = nullptr;
+      float* ds = nullptr;
+      ST_TRY(ws.get("out:i", (size_t)npairs, &di));
+      ST_TRY(ws.get("out:j", (size_t)npairs, &dj));
+      ST_TRY(ws.get("out:s", (size_t)npairs, &ds));
+      ST_TRY(launch_split_pairs(okey, oidx, osim, npairs, rbitsJ, di, dj, ds, st));
+      CU_TRY(cudaMemcpyAsync(out->i, di, sizeof(int32_t) * npairs, cudaMemcpyDeviceToHost, st));
+      CU_TRY(cudaMemcpyAsync(out->j, dj, sizeof(int32_t) * npairs, cudaMemcpyDeviceToHost, st));
+      CU_TRY(cudaMemcpyAsync(out->sim, ds, sizeof(float) * npairs, cudaMemcpyDeviceToHost, st));
+    }
+  }
+  cudaEventRecord(ctx->ev[3], st);
+  CU_TRY(cudaStreamSynchronize(st));
+  if (stats) {
+    memset(stats, 0, sizeof(*stats));
+    stats->pairs = npairs;
+    stats->candidates = ncand;
+    stats->rescored = (int64_t)hcnt[1];
+    stats->tiles = ntiles;
+    stats->head_width = SA.p;
+    stats->tail_entries = SA.ntail + (self ? 0 : SJ->ntail);
+    stats->tail_products = SA.tail_products;
+    int32_t kmax = 0;
+    if (SA.nb > 0)
+      cudaMemcpy(&kmax, SA.blk_maxnnz, sizeof(int32_t), cudaMemcpyDeviceToHost);
+    stats->max_band = ta.eps_c1 * kmax + ta.eps_c0;
+    stats->ms_preprocess = elapsed(ctx->ev[0], ctx->ev[1]);
+    stats->ms_index = 0.0;
+    stats->ms_tiles = elapsed(ctx->ev[1], ctx->ev[2]);
+    stats->ms_finalize = elapsed(ctx->ev[2], ctx->ev[3]);
+    stats->ms_total = elapsed(ctx->ev[0], ctx->ev[3]);
+    stats->launches = g_launches.load() - launches0;
+  }
+  return result;
+}
+
+}  // namespace cuapss
+
+using namespace cuapss;
+
+extern "C" {
+
+void cuapss_default_opts(cuapss_opts* o) {
+  if (!o) return;
+  memset(o, 0, sizeof(*o));
+  o->device = 0;
+  o->stream = nullptr;
+  o->precision = CUAPSS_PREC_FP32;
+  o->head_width = 0;
+  o->remap = 1;
+  o->validate = 1;
+  o->norm_tol = 1e-4f;
+  o->verbose = 0;
+}
+
+const char* cuapss_status_string(cuapss_status s) {
+  switch (s) {
+    case CUAPSS_OK: return "ok";
+    case CUAPSS_EINVAL: return "invalid argument";
+    case CUAPSS_ENOMEM: return "out of memory";
+    case CUAPSS_EOVERFLOW: return "output capacity too small";
+    case CUAPSS_ETIMEOUT: return "bounded wait timed out";
+    case CUAPSS_ECUDA: return "CUDA error";
+    case CUAPSS_EBUSY: return "admission refused";
+  }
+  return "unknown status";
+}
+
+int cuapss_abi_version(void) { return CUAPSS_ABI_VERSION; }
+
+cuapss_status cuapss_create(cuapss_ctx** out, const cuapss_opts* opts) {
+  if (!out) return CUAPSS_EINVAL;
+  *out = nullptr;
+  cuapss_opts o;
+  if (opts) o = *opts;
+  else cuapss_default_opts(&o);
+  if (o.precision != CUAPSS_PREC_FP32 && o.precision != CUAPSS_PREC_MIXED) return CUAPSS_EINVAL;
+  if (o.head_width < 0 || !(o.norm_tol >= 0.0f)) return CUAPSS_EINVAL;
+  int ndev = 0;
+  CU_TRY(cudaGetDeviceCount(&ndev));
+  if (o.device < 0 || o.device >= ndev) return CUAPSS_EINVAL;
+  CU_TRY(cudaSetDevice(o.device));
+  cuapss_ctx* c = new cuapss_ctx();
+  c->device = o.device;
+  c->opts = o;
+  cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, o.device);
+  if (o.stream) {
+    c->stream = static_cast<cudaStream_t>(o.stream);
+  } else {
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+      delete c;
+      return CUAPSS_ECUDA;
+    }
+    c->own_stream = true;
+  }
+  for (auto& e : c->ev) cudaEventCreate(&e);
+  *out = c;
+  return CUAPSS_OK;
+}
+
+cuapss_status cuapss_destroy(cuapss_ctx* c) {
+  if (!c) return CUAPSS_OK;
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->stream);
+  c->ws.release();
+  for (auto& e : c->ev)
+    if (e) cudaEventDestroy(e);
+  if (c->own_stream) cudaStreamDestroy(c->stream);
+  delete c;
+  return CUAPSS_OK;
+}
+
+cuapss_status cuapss_run(cuapss_ctx* c, const cuapss_csr* x, float t, cuapss_pairs* out,
+                         cuapss_stats* stats) {
+  if (!c) return CUAPSS_EINVAL;
+  CU_TRY(cudaSetDevice(c->device));
+  DevCsr a;
+  ST_TRY(stage_csr(c, x, "X", &a));
+  return join_device(c, a, nullptr, t, out, stats);
+}
+
+cuapss_status cuapss_join(cuapss_ctx* c, const cuapss_csr* a, const cuapss_csr* b, float t,
+                          cuapss_pairs* out, cuapss_stats* stats) {
+  if (!c) return CUAPSS_EINVAL;
+  CU_TRY(cudaSetDevice(c->device));
+  DevCsr da, db;
+  ST_TRY(stage_csr(c, a, "XA", &da));
+  ST_TRY(stage_csr(c, b, "XB", &db));
+  if (da.d != db.d) return CUAPSS_EINVAL;
+  return join_device(c, da, &db, t, out, stats);
+}
+
+cuapss_status cuapss_build_index(cuapss_ctx* c, const cuapss_csr* x, int32_t p, int32_t* dim_ptr,
+                                 int32_t* idx_row, float* idx_val, int64_t capacity,
+                                 int64_t* tail_nnz) {
+  if (!c || !dim_ptr || !tail_nnz || p < 0) return CUAPSS_EINVAL;
+  CU_TRY(cudaSetDevice(c->device));
+  DevCsr a;
+  ST_TRY(stage_csr(c, x, "IX", &a));
+  if (a.nnz >= INT32_MAX) return CUAPSS_EINVAL;
+  cudaStream_t st = c->stream;
+  ST_TRY(validate_csr(a.rp, a.col, a.val, a.n, a.d, a.nnz, 0.f, 0, nullptr, nullptr, c->ws, "IX",
+                      st));
+  int32_t* dp = nullptr;
+  ST_TRY(c->ws.get("ri:dimptr", (size_t)a.d + 1, &dp));
+  int32_t* rows = nullptr;
+  float* vals = nullptr;
+  int64_t T = 0;
+  ST_TRY(build_ref_index(a.rp, a.col, a.val, a.n, a.d, p, dp, &rows, &vals, &T, c->ws, st));
+  *tail_nnz = T;
+  if (T > capacity) {
+    CU_TRY(cudaStreamSynchronize(st));
+    return CUAPSS_EOVERFLOW;
+  }
+  if (T > 0 && (!idx_row || !idx_val)) return CUAPSS_EINVAL;
+  const cudaMemcpyKind kind = x->on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+  CU_TRY(cudaMemcpyAsync(dim_ptr, dp, sizeof(int32_t) * (a.d + 1), kind, st));
+  if (T > 0) {
+    CU_TRY(cudaMemcpyAsync(idx_row, rows, sizeof(int32_t) * T, kind, st));
+    CU_TRY(cudaMemcpyAsync(idx_val, vals, sizeof(float) * T, kind, st));
+  }
+  CU_TRY(cudaStreamSynchronize(st));
+  return CUAPSS_OK;
+}
+
+cuapss_status cuapss_feature_remap(cuapss_ctx* c, const cuapss_csr* x, int32_t* perm,
+                                   int32_t* counts) {
+  if (!c || !perm || !counts) return CUAPSS_EINVAL;
+  CU_TRY(cudaSetDevice(c->device));
+  DevCsr a;
+  ST_TRY(stage_csr(c, x, "RX", &a));
+  cudaStream_t st = c->stream;
+  int32_t* dc = nullptr;
+  int32_t* dp = nullptr;
+  ST_TRY(c->ws.get("rm:counts", (size_t)a.d, &dc));
+  ST_TRY(c->ws.get("rm:perm", (size_t)a.d, &dp));
+  CU_TRY(cudaMemsetAsync(dc, 0, sizeof(int32_t) * a.d, st));
+  ST_TRY(validate_csr(a.rp, a.col, a.val, a.n, a.d, a.nnz, 0.f, 0, dc, nullptr, c->ws, "RX", st));
+  ST_TRY(feature_perm(dc, a.d, a.n, 1, dp, c->ws, st));
+  const cudaMemcpyKind kind = x->on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+  CU_TRY(cudaMemcpyAsync(perm, dp, sizeof(int32_t) * a.d, kind, st));
+  CU_TRY(cudaMemcpyAsync(counts, dc, sizeof(int32_t) * a.d, kind, st));
+  CU_TRY(cudaStreamSynchronize(st));
+  return CUAPSS_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,44 @@
+// Context object behind the C ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+
+#include "common.cuh"
+#include "cuapss.h"
+#include "side.cuh"
+
+struct cuapss_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  cuapss_opts opts{};
+  int sms = 148;
+  cuapss::Workspace ws;
+  cudaEvent_t ev[6] = {};
+  int64_t cand_cap = 0;
+};
+
+namespace cuapss {
+
+struct DevCsr {
+  int64_t n = 0, d = 0, nnz = 0;
+  const int64_t* rp = nullptr;
+  const int32_t* col = nullptr;
+  const float* val = nullptr;
+};
+
+// Validates the descriptor and returns device pointers (staging host
+// arrays into workspace buffers named by tag).
+cuapss_status stage_csr(cuapss_ctx* ctx, const cuapss_csr* x, const std::string& tag,
+                        DevCsr* out);
+
+// The self-join (b == nullptr) or cross-join of staged matrices.
+cuapss_status join_device(cuapss_ctx* ctx, const DevCsr& a, const DevCsr* b, float t,
+                          cuapss_pairs* out, cuapss_stats* stats);
+
+// Head width used when the options leave it to the library.
+int choose_head_width(int precision, int64_t n, int64_t d, int64_t nnz);
+
+}  // namespace cuapss

@@ -1,0 +1,486 @@
+// Validation, frequency remap, row ordering, head block and inverted-list
+// build for one join operand.
+//
+// Reference counterparts (fengyilin118/APSS-CUDA):
+//  - per-row head norm pre_norm (main.cu:308-312, 324-325): FP64 sum of
+//    squares of the head entries, here computed on the device for both the
+//    head and the tail of each row, after the frequency remap;
+//  - inverted index: generate_index_ptr4 (similarity_search.cu:105-191)
+//    counts postings with atomics, the host scans the counts (1168-1186) and
+//    construct_Index2 (221-274) scatters through an atomic cursor, so list
+//    order is nondeterministic. Here the tail postings are sorted by
+//    (feature, row) with an LSD radix sort and the list pointers come from a
+//    device exclusive scan of the counts: lists are deterministic and sorted
+//    by row (the canonical form of the reference's index);
+//  - the reference fixes the head to feature ids < 4096 (similarity_search.cu
+//    :130, 250, 454, 890, ...); here features are first ranked by frequency
+//    and the head is the p most frequent ones.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+
+#include "prep.cuh"
+#include "prims.cuh"
+
+namespace cuapss {
+
+namespace {
+
+constexpr int kThreads = 256;
+
+__device__ __forceinline__ int warp_sum_i(int v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ double warp_sum_d(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ int warp_or(int v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v |= __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+__global__ void k_check_rowptr(const int64_t* __restrict__ rp, int64_t n, int64_t nnz, int* err) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i <= n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t v = rp[i];
+    int bad = 0;
+    if (v < 0 || v > nnz) bad = 1;
+    if (i == 0 && v != 0) bad = 1;
+    if (i == n && v != nnz) bad = 1;
+    if (i < n && rp[i + 1] < v) bad = 1;
+    if (bad) atomicOr(err, kErrRowptr);
+  }
+}
+
+// One warp per row: id range/order, finite values, FP64 norm, posting counts.
+__global__ void k_check_rows(const int64_t* __restrict__ rp, const int32_t* __restrict__ col,
+                             const float* __restrict__ val, int64_t n, int64_t d, float tol,
+                             int check, int32_t* __restrict__ counts, int* err,
+                             unsigned long long* nrm_max_bits) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; i < n; i += warps) {
+    const int64_t lo = rp[i], hi = rp[i + 1];
+    double ss = 0.0;
+    int bad = 0;
+    for (int64_t e = lo + lane; e < hi; e += 32) {
+      const int32_t c = col[e];
+      const float v = val[e];
+      if (c < 0 || c >= d) bad |= kErrColRange;
+      if (e > lo && col[e - 1] >= c) bad |= kErrColOrder;
+      if (!isfinite(v)) bad |= kErrValue;
+      ss += (double)v * (double)v;
+      if (counts && c >= 0 && c < d) atomicAdd(&counts[c], 1);
+    }
+    ss = warp_sum_d(ss);
+    bad = warp_or(bad);
+    if (lane == 0) {
+      const double nrm = sqrt(ss);
+      if (check && hi > lo && fabs(nrm - 1.0) > (double)tol) bad |= kErrNorm;
+      if (!check) bad &= ~kErrNorm;
+      if (bad) atomicOr(err, bad);
+      atomicMax(nrm_max_bits, (unsigned long long)__double_as_longlong(nrm));
+    }
+  }
+}
+
+__global__ void k_feat_keys(const int32_t* __restrict__ counts, int64_t d, int64_t max_count,
+                            int fbits, uint64_t* __restrict__ keys, uint32_t* __restrict__ vals) {
+  for (int64_t f = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; f < d;
+       f += (int64_t)gridDim.x * blockDim.x) {
+    keys[f] = ((uint64_t)(max_count - counts[f]) << fbits) | (uint64_t)f;
+    vals[f] = (uint32_t)f;
+  }
+}
+
+__global__ void k_perm_from_sorted(const uint32_t* __restrict__ sorted_f, int64_t d,
+                                   int32_t* __restrict__ perm) {
+  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < d;
+       r += (int64_t)gridDim.x * blockDim.x)
+    perm[sorted_f[r]] = (int32_t)r;
+}
+
+__global__ void k_iota_i32(int32_t* v, int64_t n) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    v[i] = (int32_t)i;
+}
+
+__global__ void k_row_keys(const int64_t* __restrict__ rp, int64_t n, int64_t d, int rbits,
+                           uint64_t* __restrict__ keys, uint32_t* __restrict__ vals) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t len = rp[i + 1] - rp[i];
+    keys[i] = ((uint64_t)(d - len) << rbits) | (uint64_t)i;
+    vals[i] = (uint32_t)i;
+  }
+}
+
+__global__ void k_rowperm(const uint32_t* __restrict__ sorted_rows, const int64_t* __restrict__ rp,
+                          int64_t n, int32_t* __restrict__ rowperm, int32_t* __restrict__ rowinv,
+                          int64_t* __restrict__ newlen) {
+  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n;
+       r += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t old = (int32_t)sorted_rows[r];
+    rowperm[r] = old;
+    rowinv[old] = (int32_t)r;
+    newlen[r] = rp[old + 1] - rp[old];
+  }
+}
+
+// One warp per caller row: key (new row, remapped feature) per entry.
+__global__ void k_entry_keys(const int64_t* __restrict__ rp, const int32_t* __restrict__ col,
+                             const int32_t* __restrict__ perm, const int32_t* __restrict__ rowinv,
+                             int64_t n, int fbits, uint64_t* __restrict__ keys,
+                             uint32_t* __restrict__ vals) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; i < n; i += warps) {
+    const uint64_t r = (uint64_t)rowinv[i];
+    for (int64_t e = rp[i] + lane; e < rp[i + 1]; e += 32) {
+      keys[e] = (r << fbits) | (uint64_t)perm[col[e]];
+      vals[e] = (uint32_t)e;
+    }
+  }
+}
+
+__global__ void k_gather_entries(const uint64_t* __restrict__ keys, const uint32_t* __restrict__ src,
+                                 const float* __restrict__ val, int64_t nnz, uint64_t fmask,
+                                 int32_t* __restrict__ col2, float* __restrict__ val2) {
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < nnz;
+       k += (int64_t)gridDim.x * blockDim.x) {
+    col2[k] = (int32_t)(keys[k] & fmask);
+    val2[k] = val[src[k]];
+  }
+}
+
+// One warp per new row: head length, FP64 head norm, block max nnz.
+__global__ void k_row_stats(const int64_t* __restrict__ rp2, const int32_t* __restrict__ col2,
+                            const float* __restrict__ val2, int64_t n, int p,
+                            int32_t* __restrict__ hlen, int32_t* __restrict__ nnz_row,
+                            float* __restrict__ hnorm, int64_t* __restrict__ tcount,
+                            int32_t* __restrict__ blk_maxnnz) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t r = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; r < n; r += warps) {
+    const int64_t lo = rp2[r], hi = rp2[r + 1];
+    int hl = 0;
+    double hs = 0.0;
+    for (int64_t e = lo + lane; e < hi; e += 32) {
+      if (col2[e] < p) {
+        ++hl;
+        hs += (double)val2[e] * (double)val2[e];
+      }
+    }
+    hl = warp_sum_i(hl);
+    hs = warp_sum_d(hs);
+    if (lane == 0) {
+      hlen[r] = hl;
+      nnz_row[r] = (int32_t)(hi - lo);
+      hnorm[r] = __double2float_ru(sqrt(hs));
+      tcount[r] = (hi - lo) - hl;
+      atomicMax(&blk_maxnnz[r / kBlockRows], (int32_t)(hi - lo));
+    }
+  }
+}
+
+// head32[b][c][rr] = value of feature c (< p) of row 128*b + rr
+__global__ void k_head32_scatter(const int64_t* __restrict__ rp2, const int32_t* __restrict__ col2,
+                                 const float* __restrict__ val2, const int32_t* __restrict__ hlen,
+                                 int64_t n, int p, float* __restrict__ head32) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t r = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; r < n; r += warps) {
+    const int64_t lo = rp2[r];
+    const int64_t b = r / kBlockRows, rr = r % kBlockRows;
+    for (int64_t e = lo + lane; e < lo + hlen[r]; e += 32)
+      head32[(b * p + col2[e]) * kBlockRows + rr] = val2[e];
+  }
+}
+
+// One warp per new row: tail entries in row order + (feature, row) sort keys.
+__global__ void k_tail_entries(const int64_t* __restrict__ rp2, const int32_t* __restrict__ col2,
+                               const float* __restrict__ val2, const int32_t* __restrict__ hlen,
+                               const int64_t* __restrict__ tptr, int64_t n, int p, int rbits,
+                               uint32_t* __restrict__ tk, uint8_t* __restrict__ tr,
+                               float* __restrict__ tu, uint64_t* __restrict__ keys,
+                               uint32_t* __restrict__ vals, int32_t* __restrict__ ccount) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t r = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; r < n; r += warps) {
+    const int64_t lo = rp2[r] + hlen[r], hi = rp2[r + 1];
+    const int64_t t0 = tptr[r];
+    for (int64_t k = lo + lane; k < hi; k += 32) {
+      const int64_t t = t0 + (k - lo);
+      const int32_t f = col2[k] - p;
+      tk[t] = (uint32_t)k;
+      tr[t] = (uint8_t)(r % kBlockRows);
+      tu[t] = val2[k];
+      keys[t] = ((uint64_t)f << rbits) | (uint64_t)r;
+      vals[t] = (uint32_t)t;
+      atomicAdd(&ccount[f], 1);
+    }
+  }
+}
+
+__global__ void k_csc_fill(const uint64_t* __restrict__ keys, const uint32_t* __restrict__ vals,
+                           const uint32_t* __restrict__ tk, const float* __restrict__ val2,
+                           int64_t T, uint64_t rmask, uint2* __restrict__ csc,
+                           uint32_t* __restrict__ entpos) {
+  for (int64_t m = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; m < T;
+       m += (int64_t)gridDim.x * blockDim.x) {
+    const uint32_t t = vals[m];
+    csc[m] = make_uint2((uint32_t)(keys[m] & rmask), __float_as_uint(val2[tk[t]]));
+    entpos[t] = (uint32_t)m;
+  }
+}
+
+__global__ void k_tail_products(const int32_t* __restrict__ ccount, int64_t nf,
+                                unsigned long long* out) {
+  unsigned long long s = 0;
+  for (int64_t f = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; f < nf;
+       f += (int64_t)gridDim.x * blockDim.x) {
+    const unsigned long long L = (unsigned long long)ccount[f];
+    s += L * (L > 0 ? L - 1 : 0) / 2;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0 && s) atomicAdd(out, s);
+}
+
+__global__ void k_block_tail_max(const int64_t* __restrict__ tptr, int64_t n, int nb,
+                                 unsigned long long* out) {
+  for (int64_t b = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; b < nb;
+       b += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t lo = tptr[b * kBlockRows];
+    const int64_t hi = tptr[min(n, (b + 1) * kBlockRows)];
+    atomicMax(out, (unsigned long long)(hi - lo));
+  }
+}
+
+__global__ void k_link_self(const uint32_t* __restrict__ entpos, const uint32_t* __restrict__ tk,
+                            const int32_t* __restrict__ col2, const int64_t* __restrict__ cptr,
+                            int64_t T, int p, uint32_t* __restrict__ tcur0,
+                            uint32_t* __restrict__ tend) {
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < T;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t f = col2[tk[t]] - p;
+    tcur0[t] = entpos[t] + 1u;
+    tend[t] = (uint32_t)cptr[f + 1];
+  }
+}
+
+__global__ void k_link_cross(const uint32_t* __restrict__ tk, const int32_t* __restrict__ col2,
+                             const int64_t* __restrict__ cptrJ, int64_t T, int p,
+                             uint32_t* __restrict__ tcur0, uint32_t* __restrict__ tend) {
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < T;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t f = col2[tk[t]] - p;
+    tcur0[t] = (uint32_t)cptrJ[f];
+    tend[t] = (uint32_t)cptrJ[f + 1];
+  }
+}
+
+__global__ void k_widen_i32(const int32_t* __restrict__ a, int64_t* __restrict__ b, int64_t m) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < m;
+       i += (int64_t)gridDim.x * blockDim.x)
+    b[i] = a[i];
+}
+
+inline unsigned grid_for(int64_t work, int per_block) {
+  int64_t g = ceil_div(std::max<int64_t>(work, 1), per_block);
+  return (unsigned)std::min<int64_t>(g, 148 * 32);
+}
+
+}  // namespace
+
+cuapss_status validate_csr(const int64_t* rp, const int32_t* col, const float* val, int64_t n,
+                           int64_t d, int64_t nnz, float tol, int check, int32_t* counts,
+                           double* nrm_max, Workspace& ws, const std::string& tag,
+                           cudaStream_t st) {
+  int* err = nullptr;
+  unsigned long long* nm = nullptr;
+  ST_TRY(ws.get(tag + ":err", 1, &err));
+  ST_TRY(ws.get(tag + ":nrm", 1, &nm));
+  CU_TRY(cudaMemsetAsync(err, 0, sizeof(int), st));
+  CU_TRY(cudaMemsetAsync(nm, 0, sizeof(unsigned long long), st));
+  k_check_rowptr<<<grid_for(n + 1, kThreads), kThreads, 0, st>>>(rp, n, nnz, err);
+  LAUNCH_CHECK();
+  int h_err = 0;
+  CU_TRY(cudaMemcpyAsync(&h_err, err, sizeof(int), cudaMemcpyDeviceToHost, st));
+  CU_TRY(cudaStreamSynchronize(st));
+  if (h_err) return CUAPSS_EINVAL;
+  k_check_rows<<<grid_for(n * 32, kThreads), kThreads, 0, st>>>(rp, col, val, n, d, tol, check,
+                                                                counts, err, nm);
+  LAUNCH_CHECK();
+  unsigned long long h_nm = 0;
+  CU_TRY(cudaMemcpyAsync(&h_err, err, sizeof(int), cudaMemcpyDeviceToHost, st));
+  CU_TRY(cudaMemcpyAsync(&h_nm, nm, sizeof(h_nm), cudaMemcpyDeviceToHost, st));
+  CU_TRY(cudaStreamSynchronize(st));
+  if (h_err) return CUAPSS_EINVAL;
+  double v;
+  memcpy(&v, &h_nm, sizeof(v));
+  if (nrm_max) *nrm_max = v;
+  return CUAPSS_OK;
+}
+
+cuapss_status feature_perm(const int32_t* counts, int64_t d, int64_t max_count, int remap,
+                           int32_t* perm, Workspace& ws, cudaStream_t st) {
+  if (!remap) {
+    k_iota_i32<<<grid_for(d, kThreads), kThreads, 0, st>>>(perm, d);
+    LAUNCH_CHECK();
+    return CUAPSS_OK;
+  }
+  uint64_t* keys = nullptr;
+  uint32_t* vals = nullptr;
+  ST_TRY(ws.get("perm:keys", (size_t)d, &keys));
+  ST_TRY(ws.get("perm:vals", (size_t)d, &vals));
+  const int fbits = bits_for((uint64_t)d);
+  k_feat_keys<<<grid_for(d, kThreads), kThreads, 0, st>>>(counts, d, max_count, fbits, keys, vals);
+  LAUNCH_CHECK();
+  ST_TRY(radix_sort_pairs(keys, vals, d, fbits + bits_for((uint64_t)max_count), ws, "perm", st));
+  k_perm_from_sorted<<<grid_for(d, kThreads), kThreads, 0, st>>>(vals, d, perm);
+  LAUNCH_CHECK();
+  return CUAPSS_OK;
+}
+
+cuapss_status build_side(Side& s, const PrepOptions& o, const int32_t* perm, Workspace& ws,
+                         const std::string& tag, cudaStream_t st) {
+  const int64_t n = s.n, d = s.d, nnz = s.nnz;
+  if (n >= INT32_MAX || nnz >= (int64_t)UINT32_MAX - 1) return CUAPSS_EINVAL;
+  s.p = (int)std::min<int64_t>(o.p, d);
+  if (o.want_head32) s.p = (int)std::min<int64_t>(o.p, ceil_div(d, 32) * 32);
+  const int p = s.p;
+  s.nb = (int)ceil_div(n, kBlockRows);
+  const int nb = s.nb;
+  const int rbits = std::max(1, bits_for((uint64_t)n));
+  const int fbits = std::max(1, bits_for((uint64_t)d));
+  const uint64_t fmask = (fbits >= 64) ? ~0ull : ((1ull << fbits) - 1);
+  const uint64_t rmask = (1ull << rbits) - 1;
+  const std::string t = tag + ":";
+  // ---- row order (nnz descending, then id) ----
+  int32_t* rowinv = nullptr;
+  int64_t* newlen = nullptr;
+  uint64_t* rkeys = nullptr;
+  uint32_t* rvals = nullptr;
+  ST_TRY(ws.get(t + "rowperm", (size_t)n, &s.rowperm));
+  ST_TRY(ws.get(t + "rowinv", (size_t)n, &rowinv));
+  ST_TRY(ws.get(t + "newlen", (size_t)n + 1, &newlen));
+  ST_TRY(ws.get(t + "rkeys", (size_t)n, &rkeys));
+  ST_TRY(ws.get(t + "rvals", (size_t)n, &rvals));
+  k_row_keys<<<grid_for(n, kThreads), kThreads, 0, st>>>(s.rp0, n, d, rbits, rkeys, rvals);
+  LAUNCH_CHECK();
+  if (o.row_sort)
+    ST_TRY(radix_sort_pairs(rkeys, rvals, n, rbits + fbits + 1, ws, t + "rows", st));
+  k_rowperm<<<grid_for(n, kThreads), kThreads, 0, st>>>(rvals, s.rp0, n, s.rowperm, rowinv, newlen);
+  LAUNCH_CHECK();
+  ST_TRY(ws.get(t + "rp2", (size_t)n + 1, &s.rp2));
+  ST_TRY(exclusive_scan<int64_t>(newlen, s.rp2, n, s.rp2 + n, ws, t + "rp2", st));
+  // ---- remapped, row-ordered CSR via one radix sort on (new row, rank) ----
+  uint64_t* ekeys = nullptr;
+  uint32_t* evals = nullptr;
+  ST_TRY(ws.get(t + "ekeys", (size_t)nnz, &ekeys));
+  ST_TRY(ws.get(t + "evals", (size_t)nnz, &evals));
+  ST_TRY(ws.get(t + "col2", (size_t)nnz, &s.col2));
+  ST_TRY(ws.get(t + "val2", (size_t)nnz, &s.val2));
+  k_entry_keys<<<grid_for(n * 32, kThreads), kThreads, 0, st>>>(s.rp0, s.col0, perm, rowinv, n,
+                                                                fbits, ekeys, evals);
+  LAUNCH_CHECK();
+  ST_TRY(radix_sort_pairs(ekeys, evals, nnz, rbits + fbits, ws, t + "ent", st));
+  k_gather_entries<<<grid_for(nnz, kThreads), kThreads, 0, st>>>(ekeys, evals, s.val0, nnz, fmask,
+                                                                 s.col2, s.val2);
+  LAUNCH_CHECK();
+  // ---- per-row statistics ----
+  int64_t* tcount = nullptr;
+  ST_TRY(ws.get(t + "hlen", (size_t)n, &s.hlen));
+  ST_TRY(ws.get(t + "nnzrow", (size_t)n, &s.nnz_row));
+  ST_TRY(ws.get(t + "hnorm", (size_t)n, &s.hnorm));
+  ST_TRY(ws.get(t + "tcount", (size_t)n + 1, &tcount));
+  ST_TRY(ws.get(t + "blkmax", (size_t)nb + 1, &s.blk_maxnnz));
+  CU_TRY(cudaMemsetAsync(s.blk_maxnnz, 0, sizeof(int32_t) * (nb + 1), st));
+  k_row_stats<<<grid_for(n * 32, kThreads), kThreads, 0, st>>>(s.rp2, s.col2, s.val2, n, p, s.hlen,
+                                                               s.nnz_row, s.hnorm, tcount,
+                                                               s.blk_maxnnz);
+  LAUNCH_CHECK();
+  ST_TRY(ws.get(t + "tptr", (size_t)n + 1, &s.tptr));
+  ST_TRY(exclusive_scan<int64_t>(tcount, s.tptr, n, s.tptr + n, ws, t + "tptr", st));
+  // ---- dense FP32 head block ----
+  if (o.want_head32 && p > 0) {
+    const size_t hb = (size_t)nb * p * kBlockRows;
+    ST_TRY(ws.get(t + "head32", hb, &s.head32));
+    CU_TRY(cudaMemsetAsync(s.head32, 0, hb * sizeof(float), st));
+    k_head32_scatter<<<grid_for(n * 32, kThreads), kThreads, 0, st>>>(s.rp2, s.col2, s.val2,
+                                                                      s.hlen, n, p, s.head32);
+    LAUNCH_CHECK();
+  }
+  // ---- tail: entries in row order and the global inverted lists ----
+  CU_TRY(cudaMemcpyAsync(&s.ntail, s.tptr + n, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+  CU_TRY(cudaStreamSynchronize(st));
+  const int64_t T = s.ntail;
+  const int64_t nf = std::max<int64_t>(d - p, 0);
+  uint64_t* tkeys = nullptr;
+  uint32_t* tvals = nullptr;
+  int32_t* ccount = nullptr;
+  uint32_t* entpos = nullptr;
+  ST_TRY(ws.get(t + "tk", (size_t)T, &s.tk));
+  ST_TRY(ws.get(t + "tr", (size_t)T, &s.tr));
+  ST_TRY(ws.get(t + "tu", (size_t)T, &s.tu));
+  ST_TRY(ws.get(t + "tcur0", (size_t)T, &s.tcur0));
+  ST_TRY(ws.get(t + "tend", (size_t)T, &s.tend));
+  ST_TRY(ws.get(t + "tkeys", (size_t)T, &tkeys));
+  ST_TRY(ws.get(t + "tvals", (size_t)T, &tvals));
+  ST_TRY(ws.get(t + "entpos", (size_t)T, &entpos));
+  ST_TRY(ws.get(t + "ccount", (size_t)nf + 1, &ccount));
+  ST_TRY(ws.get(t + "cptr", (size_t)nf + 1, &s.cptr));
+  ST_TRY(ws.get(t + "csc", (size_t)T, &s.csc));
+  CU_TRY(cudaMemsetAsync(ccount, 0, sizeof(int32_t) * (nf + 1), st));
+  k_tail_entries<<<grid_for(n * 32, kThreads), kThreads, 0, st>>>(
+      s.rp2, s.col2, s.val2, s.hlen, s.tptr, n, p, rbits, s.tk, s.tr, s.tu, tkeys, tvals, ccount);
+  LAUNCH_CHECK();
+  ST_TRY(radix_sort_pairs(tkeys, tvals, T, rbits + std::max(1, bits_for((uint64_t)nf)), ws,
+                          t + "csc", st));
+  k_csc_fill<<<grid_for(T, kThreads), kThreads, 0, st>>>(tkeys, tvals, s.tk, s.val2, T, rmask,
+                                                        s.csc, entpos);
+  LAUNCH_CHECK();
+  {
+    // int32 counts -> int64 list pointers
+    int64_t* c64 = nullptr;
+    ST_TRY(ws.get(t + "ccount64", (size_t)nf + 1, &c64));
+    k_widen_i32<<<grid_for(nf, kThreads), kThreads, 0, st>>>(ccount, c64, nf);
+    LAUNCH_CHECK();
+    ST_TRY(exclusive_scan<int64_t>(c64, s.cptr, nf, s.cptr + nf, ws, t + "cptr", st));
+  }
+  unsigned long long* red = nullptr;
+  ST_TRY(ws.get(t + "red", 2, &red));
+  CU_TRY(cudaMemsetAsync(red, 0, 2 * sizeof(unsigned long long), st));
+  k_tail_products<<<grid_for(nf, kThreads), kThreads, 0, st>>>(ccount, nf, red);
+  LAUNCH_CHECK();
+  k_block_tail_max<<<grid_for(nb, kThreads), kThreads, 0, st>>>(s.tptr, n, nb, red + 1);
+  LAUNCH_CHECK();
+  k_link_self<<<grid_for(T, kThreads), kThreads, 0, st>>>(entpos, s.tk, s.col2, s.cptr, T, p,
+                                                         s.tcur0, s.tend);
+  LAUNCH_CHECK();
+  unsigned long long hred[2] = {0, 0};
+  CU_TRY(cudaMemcpyAsync(hred, red, sizeof(hred), cudaMemcpyDeviceToHost, st));
+  CU_TRY(cudaStreamSynchronize(st));
+  s.tail_products = (int64_t)hred[0];
+  s.max_block_tail = (int64_t)hred[1];
+  return CUAPSS_OK;
+}
+
+cuapss_status link_tail(Side& I, const Side& J, bool self, cudaStream_t st) {
+  if (self) return CUAPSS_OK;  // build_side already linked a side to itself
+  if (I.p != J.p || I.d != J.d) return CUAPSS_EINVAL;
+  k_link_cross<<<grid_for(I.ntail, kThreads), kThreads, 0, st>>>(I.tk, I.col2, J.cptr, I.ntail,
+                                                                 I.p, I.tcur0, I.tend);
+  LAUNCH_CHECK();
+  return CUAPSS_OK;
+}
+
+}  // namespace cuapss

@@ -1,0 +1,39 @@
+// Preparation of one join operand: validation, frequency remap, row order,
+// head block and inverted lists.
+#pragma once
+
+#include <string>
+
+#include "common.cuh"
+#include "side.cuh"
+
+namespace cuapss {
+
+struct PrepOptions {
+  int p = 64;           // head width (multiple of 32 for the FP32 head block)
+  int row_sort = 1;     // order rows by nnz descending
+  int want_head32 = 1;  // build the FP32 head block
+  int want_head16 = 0;  // build the BF16 head block
+};
+
+// Validates a device CSR. counts (device, d entries, may be null) are
+// incremented per posting. *nrm_max receives the largest row norm.
+cuapss_status validate_csr(const int64_t* rp, const int32_t* col, const float* val, int64_t n,
+                           int64_t d, int64_t nnz, float tol, int check, int32_t* counts,
+                           double* nrm_max, Workspace& ws, const std::string& tag,
+                           cudaStream_t st);
+
+// perm[f] = rank of feature f by (count desc, id asc); identity if !remap.
+cuapss_status feature_perm(const int32_t* counts, int64_t d, int64_t max_count, int remap,
+                           int32_t* perm, Workspace& ws, cudaStream_t st);
+
+// Builds every array of `s` (s.rp0/col0/val0/n/d/nnz must be set).
+cuapss_status build_side(Side& s, const PrepOptions& o, const int32_t* perm, Workspace& ws,
+                         const std::string& tag, cudaStream_t st);
+
+// Points the tail cursors of `I` at the inverted lists of `J` (same remap and
+// p). self: I and J are the same side and each entry starts after its own
+// posting, so only pairs i < j are visited.
+cuapss_status link_tail(Side& I, const Side& J, bool self, cudaStream_t st);
+
+}  // namespace cuapss

@@ -1,0 +1,65 @@
+// Device-resident layout of one operand of a similarity join, after
+// validation, frequency remap, row ordering and the index build.
+//
+// HBM layout (n rows, d features, nnz non-zeros, p head width, nb = ceil(n/128)
+// row blocks of 128 rows, T tail non-zeros):
+//   rowperm   int32[n]        new row -> caller's row (rows ordered by nnz
+//                             descending, then id)
+//   rp2       int64[n+1]      CSR of the remapped, row-ordered matrix
+//   col2/val2 int32/f32[nnz]  feature ids remapped by frequency rank, sorted
+//                             ascending in each row: the head (rank < p) is a
+//                             row prefix of length hlen[r]
+//   head32    f32[nb][p][128] dense head block, k-major inside a row block so
+//                             that a 32-feature slice of a block is one
+//                             contiguous 16 KB run (one bulk TMA copy)
+//   head16    bf16            dense head block for the tensor-core path
+//   cptr/csc  int64[d-p+1], {int32 row, f32 val}[T]
+//                             inverted lists of the tail features (rank >= p),
+//                             rows ascending: the global index
+//   tptr      int64[n+1]      tail entries of each row, in row order
+//   tcur0/tend/tr/tu          per tail entry: first posting to visit in the
+//                             J-side index, end of that list, row inside its
+//                             block, value
+#pragma once
+
+#include <cuda_bf16.h>
+
+#include <cstdint>
+
+#include "common.cuh"
+
+namespace cuapss {
+
+struct Side {
+  int64_t n = 0, d = 0, nnz = 0;
+  int nb = 0;       // row blocks of kBlockRows
+  int p = 0;        // head width
+  // caller's CSR on the device (input pointers or a staged copy)
+  const int64_t* rp0 = nullptr;
+  const int32_t* col0 = nullptr;
+  const float* val0 = nullptr;
+  int32_t* rowperm = nullptr;
+  int64_t* rp2 = nullptr;
+  int32_t* col2 = nullptr;
+  float* val2 = nullptr;
+  int32_t* hlen = nullptr;
+  int32_t* nnz_row = nullptr;
+  int32_t* blk_maxnnz = nullptr;  // [nb]
+  float* hnorm = nullptr;         // head norm (rounded up), new row order
+  float* head32 = nullptr;
+  __nv_bfloat16* head16 = nullptr;
+  int64_t* tptr = nullptr;
+  uint32_t* tk = nullptr;         // tail entry -> index into col2/val2
+  int64_t* cptr = nullptr;
+  uint2* csc = nullptr;
+  uint32_t* tcur0 = nullptr;
+  uint32_t* tend = nullptr;
+  uint8_t* tr = nullptr;
+  float* tu = nullptr;
+  int64_t ntail = 0;
+  int64_t max_block_tail = 0;
+  int64_t tail_products = 0;      // sum over tail lists of L(L-1)/2
+  double nrm_max = 1.0;           // largest row norm (FP64)
+};
+
+}  // namespace cuapss

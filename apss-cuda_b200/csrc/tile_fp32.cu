@@ -1,0 +1,264 @@
+// Plain FP32 hybrid pair-tile kernel.
+//
+// One CTA evaluates 128 x 128 pair tiles (I block of rows x J block of
+// columns) of the similarity matrix:
+//  1. tail, feature-parallel: every tail posting (row r of I, feature f,
+//     value u) keeps a cursor into the inverted list of f in the J-side
+//     index; postings of f whose row falls in J are consumed and
+//     u * v is added into a shared-memory accumulator acc[r][c] with
+//     shared-memory atomics (the role of similarity_apss1 /
+//     similarity_join1, fengyilin118/APSS-CUDA similarity_search.cu:370-437
+//     and 642-735, which instead add into a dense n x n global array);
+//  2. head, pair-parallel: the dense head blocks of I and J (p features, 32
+//     at a time, one 16 KB bulk-TMA copy per operand and slice, double
+//     buffered) are multiplied with an FP32 FMA chain, 8 x 8 pairs per
+//     thread (the role of similarity_apss_rest / similarity_join_rest,
+//     similarity_search.cu:441-506 and 854-915, which do a sparse-dense dot
+//     per pair against a dense copy of the query's head);
+//  3. epilogue: head + tail is compared with t - eps (eps bounds the FP32
+//     rounding of the tile, so no pair with FP64 similarity >= t is lost;
+//     the reference's prune filter_pair, 510-531, uses "<= t" and drops
+//     pairs at exactly t); surviving pairs are compacted with a warp ballot
+//     and one atomic per warp into the candidate list (the reference counts
+//     nothing: its atomicAdd(sum_pair) is commented out, 501 and 910).
+// Units of work are taken from a global counter (persistent CTAs).
+#include <cuda_runtime.h>
+
+#include <climits>
+
+#include "ptx.cuh"
+#include "tiles.cuh"
+
+namespace cuapss {
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kKC = 32;                           // head features per slice
+constexpr int kSlice = kKC * kBlockRows;          // floats per slice (4096)
+constexpr int kSliceBytes = kSlice * 4;           // 16 KB
+constexpr int kAccLd = kBlockRows + 4;            // padded accumulator row
+constexpr size_t kSmemBytes = 4 * (size_t)kSliceBytes + (size_t)kBlockRows * kAccLd * 4 + 64;
+
+struct Smem {
+  float* a[2];
+  float* b[2];
+  float* acc;
+  uint64_t* bar;
+};
+
+__device__ __forceinline__ Smem carve(unsigned char* base) {
+  Smem s;
+  s.a[0] = reinterpret_cast<float*>(base);
+  s.a[1] = s.a[0] + kSlice;
+  s.b[0] = s.a[1] + kSlice;
+  s.b[1] = s.b[0] + kSlice;
+  s.acc = s.b[1] + kSlice;
+  s.bar = reinterpret_cast<uint64_t*>(s.acc + kBlockRows * kAccLd);
+  return s;
+}
+
+__device__ __forceinline__ void issue_slice(const Smem& s, int stage, const float* headI,
+                                            const float* headJ, int I, int J, int p, int kc) {
+  mbar_arrive_expect_tx(&s.bar[stage], 2 * kSliceBytes);
+  bulk_g2s(s.a[stage], headI + ((int64_t)I * p + (int64_t)kc * kKC) * kBlockRows, kSliceBytes,
+           &s.bar[stage]);
+  bulk_g2s(s.b[stage], headJ + ((int64_t)J * p + (int64_t)kc * kKC) * kBlockRows, kSliceBytes,
+           &s.bar[stage]);
+}
+
+__global__ void __launch_bounds__(kThreads, 1) k_tiles_fp32(const TileArgs A) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  const Smem S = carve(smem_raw);
+  __shared__ int s_unit;
+  const int tid = threadIdx.x;
+  const int ty = tid >> 4, tx = tid & 15;
+  const int lane = tid & 31;
+  if (tid == 0) {
+    mbar_init(&S.bar[0], 1);
+    mbar_init(&S.bar[1], 1);
+    fence_mbar_init();
+  }
+  for (int i = tid; i < kBlockRows * kAccLd; i += kThreads) S.acc[i] = 0.0f;
+  __syncthreads();
+  uint32_t parity[2] = {0u, 0u};
+  const int nchunks = A.p / kKC;
+  uint32_t* scr_cur = A.scr_cur + (int64_t)blockIdx.x * A.scr_stride;
+  uint32_t* scr_next = A.scr_next + (int64_t)blockIdx.x * A.scr_stride;
+
+  for (;;) {
+    if (tid == 0) s_unit = atomicAdd(A.unit_counter, 1);
+    __syncthreads();
+    const int u = s_unit;
+    __syncthreads();
+    if (u >= A.nunits) break;
+    int blocks[2];
+    int nblk;
+    if (A.self) {
+      blocks[0] = u;
+      blocks[1] = A.nbI - 1 - u;
+      nblk = blocks[1] != blocks[0] ? 2 : 1;
+    } else {
+      blocks[0] = u;
+      nblk = 1;
+    }
+    for (int bi = 0; bi < nblk; ++bi) {
+      const int I = blocks[bi];
+      const int64_t row0 = (int64_t)I * kBlockRows;
+      const int rowsI = (int)(A.nI - row0 < kBlockRows ? A.nI - row0 : kBlockRows);
+      const int64_t e0 = A.tptrI[row0];
+      const int ne = (int)(A.tptrI[row0 + rowsI] - e0);
+      if (ne > A.scr_stride) {  // sized by the host from the largest block
+        if (tid == 0) atomicOr(A.err, kErrInternal);
+        return;
+      }
+      for (int e = tid; e < ne; e += kThreads) {
+        const uint32_t c = A.tcur0[e0 + e], end = A.tend[e0 + e];
+        scr_cur[e] = c;
+        scr_next[e] = c < end ? A.cscJ[c].x : 0xffffffffu;
+      }
+      __syncthreads();
+      const int Jbeg = A.self ? I : 0;
+      for (int J = Jbeg; J < A.nbJ; ++J) {
+        const int64_t col0 = (int64_t)J * kBlockRows;
+        const uint32_t j0 = (uint32_t)col0, j1 = (uint32_t)(col0 + kBlockRows);
+        if (tid == 0 && nchunks > 0) issue_slice(S, 0, A.headI32, A.headJ32, I, J, A.p, 0);
+        // ---- tail: consume the postings of I's tail features that fall in J
+        for (int e = tid; e < ne; e += kThreads) {
+          uint32_t nr = scr_next[e];
+          if (nr < j1) {
+            const int r = A.tr[e0 + e];
+            const float uval = A.tu[e0 + e];
+            uint32_t cur = scr_cur[e];
+            const uint32_t end = A.tend[e0 + e];
+            uint2 pst = A.cscJ[cur];
+            for (;;) {
+              atomicAdd(&S.acc[r * kAccLd + (int)(pst.x - j0)], uval * __uint_as_float(pst.y));
+              ++cur;
+              if (cur >= end) {
+                nr = 0xffffffffu;
+                break;
+              }
+              pst = A.cscJ[cur];
+              if (pst.x >= j1) {
+                nr = pst.x;
+                break;
+              }
+            }
+            scr_cur[e] = cur;
+            scr_next[e] = nr;
+          }
+        }
+        // ---- head: FP32 FMA chain over the p head features
+        float h[8][8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i)
+#pragma unroll
+          for (int j = 0; j < 8; ++j) h[i][j] = 0.0f;
+        for (int kc = 0; kc < nchunks; ++kc) {
+          const int stage = kc & 1;
+          if (tid == 0 && kc + 1 < nchunks)
+            issue_slice(S, stage ^ 1, A.headI32, A.headJ32, I, J, A.p, kc + 1);
+          const bool ok = mbar_wait(&S.bar[stage], parity[stage]);
+          parity[stage] ^= 1u;
+          if (__syncthreads_or(!ok)) {
+            if (tid == 0) atomicOr(A.err, kErrTimeout);
+            return;
+          }
+          const float4* a4 = reinterpret_cast<const float4*>(S.a[stage]);
+          const float4* b4 = reinterpret_cast<const float4*>(S.b[stage]);
+#pragma unroll 8
+          for (int k = 0; k < kKC; ++k) {
+            const float4 a0 = a4[k * 32 + ty], a1 = a4[k * 32 + 16 + ty];
+            const float4 b0 = b4[k * 32 + tx], b1 = b4[k * 32 + 16 + tx];
+            const float av[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
+            const float bv[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+#pragma unroll
+            for (int i = 0; i < 8; ++i)
+#pragma unroll
+              for (int j = 0; j < 8; ++j) h[i][j] = fmaf(av[i], bv[j], h[i][j]);
+          }
+          __syncthreads();
+        }
+        if (nchunks == 0) __syncthreads();
+        // ---- epilogue: head + tail >= t - eps  ->  candidates
+        const int colsJ = (int)(A.nJ - col0 < kBlockRows ? A.nJ - col0 : kBlockRows);
+        const bool diag = A.self && (I == J);
+        const int kmax = min(A.blkmaxI[I], A.blkmaxJ[J]);
+        const float t_lo = __double2float_rd((double)A.t - (A.eps_c1 * kmax + A.eps_c0));
+        unsigned long long pass = 0ull;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+          const int r = (i < 4) ? ty * 4 + i : 64 + ty * 4 + (i - 4);
+          float4* arow = reinterpret_cast<float4*>(S.acc + r * kAccLd);
+          const float4 t0 = arow[tx], t1 = arow[16 + tx];
+          arow[tx] = make_float4(0.f, 0.f, 0.f, 0.f);
+          arow[16 + tx] = make_float4(0.f, 0.f, 0.f, 0.f);
+          const float tv[8] = {t0.x, t0.y, t0.z, t0.w, t1.x, t1.y, t1.z, t1.w};
+#pragma unroll
+          for (int j = 0; j < 8; ++j) {
+            const int c = (j < 4) ? tx * 4 + j : 64 + tx * 4 + (j - 4);
+            const float s = h[i][j] + tv[j];
+            h[i][j] = s;
+            const bool ok = (s >= t_lo) && (r < rowsI) && (c < colsJ) && (!diag || c > r);
+            pass |= (unsigned long long)ok << (i * 8 + j);
+          }
+        }
+        if (__any_sync(0xffffffffu, pass != 0ull)) {
+          const int mine = __popcll(pass);
+          int incl = mine;
+#pragma unroll
+          for (int o = 1; o < 32; o <<= 1) {
+            const int v = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += v;
+          }
+          const int total = __shfl_sync(0xffffffffu, incl, 31);
+          unsigned long long base = 0;
+          if (lane == 31) base = atomicAdd(A.cand_count, (unsigned long long)total);
+          base = __shfl_sync(0xffffffffu, base, 31);
+          unsigned long long w = base + (unsigned long long)(incl - mine);
+#pragma unroll
+          for (int i = 0; i < 8; ++i) {
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+              if ((pass >> (i * 8 + j)) & 1ull) {
+                const int r = (i < 4) ? ty * 4 + i : 64 + ty * 4 + (i - 4);
+                const int c = (j < 4) ? tx * 4 + j : 64 + tx * 4 + (j - 4);
+                if ((int64_t)w < A.cand_cap) {
+                  A.cand_key[w] = ((uint64_t)(row0 + r) << 32) | (uint64_t)(col0 + c);
+                  A.cand_sim[w] = h[i][j];
+                }
+                ++w;
+              }
+            }
+          }
+        }
+        __syncthreads();  // accumulator cleared, cursors advanced
+      }
+    }
+  }
+}
+
+}  // namespace
+
+int tiles_fp32_max_grid() {
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  return sms;
+}
+
+cuapss_status launch_tiles_fp32(const TileArgs& a, int grid, cudaStream_t st) {
+  static bool attr_set = false;
+  if (!attr_set) {
+    CU_TRY(cudaFuncSetAttribute(k_tiles_fp32, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)kSmemBytes));
+    attr_set = true;
+  }
+  if (a.p % kKC != 0) return CUAPSS_EINVAL;
+  k_tiles_fp32<<<grid, kThreads, kSmemBytes, st>>>(a);
+  LAUNCH_CHECK();
+  return CUAPSS_OK;
+}
+
+}  // namespace cuapss

@@ -1,0 +1,96 @@
+// Launch interfaces of the pair-tile kernels and the finalize stage.
+#pragma once
+
+#include <cstdint>
+
+#include "common.cuh"
+#include "side.cuh"
+
+namespace cuapss {
+
+// Arguments shared by the pair-tile kernels. A "unit" is the work one CTA
+// takes from the global counter: for a self-join the row-block pair
+// (u, nb-1-u) (so every unit holds nb+1 tiles of the upper triangle), for a
+// cross-join one I block against every J block.
+struct TileArgs {
+  // I side (rows of the tile)
+  const float* headI32;
+  const void* headI16;
+  int64_t nI;
+  int nbI;
+  const int64_t* tptrI;
+  const uint32_t* tcur0;
+  const uint32_t* tend;
+  const uint8_t* tr;
+  const float* tu;
+  const int32_t* blkmaxI;
+  const float* hnormI;
+  // J side (columns of the tile)
+  const float* headJ32;
+  const void* headJ16;
+  int64_t nJ;
+  int nbJ;
+  const uint2* cscJ;
+  const int32_t* blkmaxJ;
+  const float* hnormJ;
+  int p;
+  int self;
+  float t;
+  double eps_c1;  // FP32 error margin of a tile: eps_c1 * min(maxnnz_I, maxnnz_J) + eps_c0
+  double eps_c0;
+  double eps_head;  // tensor-core path: extra margin per unit of ||a_h|| ||b_h||
+  int nunits;
+  int* unit_counter;
+  uint32_t* scr_cur;
+  uint32_t* scr_next;
+  int64_t scr_stride;
+  uint64_t* cand_key;
+  float* cand_sim;
+  unsigned long long* cand_count;
+  int64_t cand_cap;
+  int* err;
+};
+
+// Plain FP32 hybrid tile kernel (head: FP32 forward-list dot on TMA-staged
+// row tiles; tail: inverted-list scan into shared-memory accumulators).
+cuapss_status launch_tiles_fp32(const TileArgs& a, int grid, cudaStream_t st);
+int tiles_fp32_max_grid();
+
+struct FinalizeArgs {
+  const uint64_t* cand_key;
+  const float* cand_sim;
+  int64_t ncand;
+  const int32_t* rowpermI;
+  const int32_t* rowpermJ;
+  const int32_t* nnzI;
+  const int32_t* nnzJ;
+  const float* hnormI;
+  const float* hnormJ;
+  const int64_t* rpI;
+  const int32_t* colI;
+  const float* valI;
+  const int64_t* rpJ;
+  const int32_t* colJ;
+  const float* valJ;
+  float t;
+  double eps_c1;
+  double eps_c0;
+  double eps_head;
+  int self;
+  int rbits;  // output key = (i << rbits) | j
+  uint64_t* out_key;
+  uint32_t* out_idx;
+  float* out_sim;
+  unsigned long long* out_count;
+  int64_t out_cap;
+  unsigned long long* n_rescored;
+};
+
+cuapss_status launch_finalize(const FinalizeArgs& a, cudaStream_t st);
+
+// After sorting out_key (with out_idx as payload): split into i, j, sim.
+cuapss_status launch_split_pairs(const uint64_t* key, const uint32_t* idx, const float* sim_in,
+                                 int64_t m, int rbits, int32_t* oi, int32_t* oj, float* os,
+                                 cudaStream_t st);
+
+}  // namespace cuapss

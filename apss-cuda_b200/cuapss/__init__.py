@@ -1,0 +1,262 @@
+"""Python host binding of the CuAPSS C ABI (include/cuapss.h).
+
+Mirrors the reference's one entry point -- similarity_join_device
+(fengyilin118/APSS-CUDA similarity_search.h:3-14), which takes the
+pre-processed vectors and reports the pairs whose cosine similarity is >= the
+threshold -- as a context object with ``run`` (self-join), ``join``
+(cross-join), ``build_index`` (the reference's inverted index) and
+``feature_remap``. All compute happens in ``lib/libcuapss.so``; if the
+library is missing this module raises instead of falling back to anything.
+
+Inputs are :class:`cuapss.synth.Csr` host matrices (numpy) or dictionaries
+of CUDA torch tensors ``{"rowptr", "col", "val", "d"}`` (device pointers are
+then passed straight through).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+from .synth import Csr, CONFIGS, SynthConfig, generate  # noqa: F401
+
+_LIB_DIR = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "lib")
+LIB_PATH = os.path.join(_LIB_DIR, "libcuapss.so")
+
+OK, EINVAL, ENOMEM, EOVERFLOW, ETIMEOUT, ECUDA, EBUSY = range(7)
+PREC_FP32, PREC_MIXED = 0, 1
+
+
+class CuapssError(RuntimeError):
+    def __init__(self, status: int, what: str):
+        self.status = status
+        super().__init__(f"{what}: {status_string(status)} ({status})")
+
+
+class Opts(ctypes.Structure):
+    _fields_ = [
+        ("device", ctypes.c_int),
+        ("stream", ctypes.c_void_p),
+        ("precision", ctypes.c_int),
+        ("head_width", ctypes.c_int),
+        ("remap", ctypes.c_int),
+        ("validate", ctypes.c_int),
+        ("norm_tol", ctypes.c_float),
+        ("verbose", ctypes.c_int),
+    ]
+
+
+class CsrDesc(ctypes.Structure):
+    _fields_ = [
+        ("n", ctypes.c_int64),
+        ("d", ctypes.c_int64),
+        ("nnz", ctypes.c_int64),
+        ("rowptr", ctypes.c_void_p),
+        ("col", ctypes.c_void_p),
+        ("val", ctypes.c_void_p),
+        ("on_device", ctypes.c_int),
+    ]
+
+
+class PairsDesc(ctypes.Structure):
+    _fields_ = [
+        ("i", ctypes.c_void_p),
+        ("j", ctypes.c_void_p),
+        ("sim", ctypes.c_void_p),
+        ("capacity", ctypes.c_int64),
+        ("count", ctypes.c_int64),
+        ("on_device", ctypes.c_int),
+    ]
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [
+        ("pairs", ctypes.c_int64),
+        ("candidates", ctypes.c_int64),
+        ("rescored", ctypes.c_int64),
+        ("tiles", ctypes.c_int64),
+        ("head_width", ctypes.c_int64),
+        ("tail_entries", ctypes.c_int64),
+        ("tail_products", ctypes.c_int64),
+        ("max_band", ctypes.c_double),
+        ("ms_preprocess", ctypes.c_double),
+        ("ms_index", ctypes.c_double),
+        ("ms_tiles", ctypes.c_double),
+        ("ms_finalize", ctypes.c_double),
+        ("ms_total", ctypes.c_double),
+        ("launches", ctypes.c_int64),
+    ]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+_P = ctypes.c_void_p
+_lib = None
+
+# Every symbol declared by include/cuapss.h (checked by the CPU tests).
+EXPORTED = [
+    "cuapss_default_opts", "cuapss_status_string", "cuapss_abi_version", "cuapss_create",
+    "cuapss_destroy", "cuapss_run", "cuapss_join", "cuapss_build_index", "cuapss_feature_remap",
+]
+
+
+def lib():
+    """Load lib/libcuapss.so (raises if it is not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is not built; run __graft_entry__.build()")
+        L = ctypes.CDLL(LIB_PATH)
+        L.cuapss_default_opts.argtypes = [ctypes.POINTER(Opts)]
+        L.cuapss_default_opts.restype = None
+        L.cuapss_status_string.argtypes = [ctypes.c_int]
+        L.cuapss_status_string.restype = ctypes.c_char_p
+        L.cuapss_abi_version.restype = ctypes.c_int
+        L.cuapss_create.argtypes = [ctypes.POINTER(_P), ctypes.POINTER(Opts)]
+        L.cuapss_create.restype = ctypes.c_int
+        L.cuapss_destroy.argtypes = [_P]
+        L.cuapss_destroy.restype = ctypes.c_int
+        L.cuapss_run.argtypes = [_P, ctypes.POINTER(CsrDesc), ctypes.c_float,
+                                 ctypes.POINTER(PairsDesc), ctypes.POINTER(Stats)]
+        L.cuapss_run.restype = ctypes.c_int
+        L.cuapss_join.argtypes = [_P, ctypes.POINTER(CsrDesc), ctypes.POINTER(CsrDesc),
+                                  ctypes.c_float, ctypes.POINTER(PairsDesc),
+                                  ctypes.POINTER(Stats)]
+        L.cuapss_join.restype = ctypes.c_int
+        L.cuapss_build_index.argtypes = [_P, ctypes.POINTER(CsrDesc), ctypes.c_int32, _P, _P, _P,
+                                         ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)]
+        L.cuapss_build_index.restype = ctypes.c_int
+        L.cuapss_feature_remap.argtypes = [_P, ctypes.POINTER(CsrDesc), _P, _P]
+        L.cuapss_feature_remap.restype = ctypes.c_int
+        _lib = L
+    return _lib
+
+
+def status_string(s: int) -> str:
+    return lib().cuapss_status_string(int(s)).decode()
+
+
+def default_opts() -> Opts:
+    o = Opts()
+    lib().cuapss_default_opts(ctypes.byref(o))
+    return o
+
+
+def _check(status: int, what: str) -> None:
+    if status != OK:
+        raise CuapssError(status, what)
+
+
+def _desc(x) -> tuple:
+    """(CsrDesc, keepalive) for a host Csr or a dict of CUDA tensors."""
+    if isinstance(x, Csr):
+        d = CsrDesc(x.n, x.d, x.nnz, x.rowptr.ctypes.data, x.col.ctypes.data,
+                    x.val.ctypes.data, 0)
+        return d, x
+    rp, col, val = x["rowptr"], x["col"], x["val"]
+    d = CsrDesc(int(rp.numel()) - 1, int(x["d"]), int(col.numel()), rp.data_ptr(),
+                col.data_ptr(), val.data_ptr(), 1)
+    return d, x
+
+
+class Context:
+    """One CuAPSS context (one device, one stream, one host thread at a time)."""
+
+    def __init__(self, device: int = 0, precision: int = PREC_FP32, head_width: int = 0,
+                 remap: bool = True, validate: bool = True, norm_tol: float = 1e-4,
+                 stream: int | None = None):
+        o = default_opts()
+        o.device = device
+        o.precision = precision
+        o.head_width = head_width
+        o.remap = 1 if remap else 0
+        o.validate = 1 if validate else 0
+        o.norm_tol = norm_tol
+        o.stream = stream
+        self._h = _P()
+        _check(lib().cuapss_create(ctypes.byref(self._h), ctypes.byref(o)), "cuapss_create")
+        self.last_stats: dict = {}
+
+    def close(self) -> None:
+        if self._h:
+            lib().cuapss_destroy(self._h)
+            self._h = _P()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _pairs_call(self, fn, args, capacity: int):
+        cap = max(int(capacity), 1)
+        while True:
+            oi = np.empty(cap, np.int32)
+            oj = np.empty(cap, np.int32)
+            os_ = np.empty(cap, np.float32)
+            pr = PairsDesc(oi.ctypes.data, oj.ctypes.data, os_.ctypes.data, cap, 0, 0)
+            st = Stats()
+            s = fn(self._h, *args, ctypes.byref(pr), ctypes.byref(st))
+            if s == EOVERFLOW:
+                cap = int(pr.count)
+                continue
+            _check(s, fn.__name__)
+            self.last_stats = st.as_dict()
+            n = int(pr.count)
+            return oi[:n].copy(), oj[:n].copy(), os_[:n].copy()
+
+    def run(self, x, t: float, capacity: int = 1 << 16):
+        """Self-join: (i, j, sim) numpy arrays, i < j, sorted by (i, j)."""
+        d, keep = _desc(x)
+        return self._pairs_call(lib().cuapss_run, (ctypes.byref(d), ctypes.c_float(t)), capacity)
+
+    def run_device(self, x, t: float, out: dict):
+        """Self-join into CUDA tensors out = {"i", "j", "sim"}; returns the
+        pair count (raises CuapssError(EOVERFLOW) with .status if short)."""
+        d, keep = _desc(x)
+        cap = int(out["i"].numel())
+        pr = PairsDesc(out["i"].data_ptr(), out["j"].data_ptr(), out["sim"].data_ptr(), cap, 0, 1)
+        st = Stats()
+        s = lib().cuapss_run(self._h, ctypes.byref(d), ctypes.c_float(t), ctypes.byref(pr),
+                             ctypes.byref(st))
+        self.last_stats = st.as_dict()
+        if s == EOVERFLOW:
+            self.required = int(pr.count)
+        _check(s, "cuapss_run")
+        return int(pr.count)
+
+    def join(self, a, b, t: float, capacity: int = 1 << 16):
+        """Cross-join: (i in a, j in b, sim), sorted by (i, j)."""
+        da, ka = _desc(a)
+        db, kb = _desc(b)
+        return self._pairs_call(lib().cuapss_join,
+                                (ctypes.byref(da), ctypes.byref(db), ctypes.c_float(t)), capacity)
+
+    def build_index(self, x: Csr, p: int):
+        """Reference-semantics tail index: (dim_ptr[d+1], rows, vals)."""
+        d, keep = _desc(x)
+        dim_ptr = np.empty(x.d + 1, np.int32)
+        cap = max(int((x.col >= p).sum()), 1)
+        rows = np.empty(cap, np.int32)
+        vals = np.empty(cap, np.float32)
+        tn = ctypes.c_int64()
+        _check(lib().cuapss_build_index(self._h, ctypes.byref(d), int(p), dim_ptr.ctypes.data,
+                                        rows.ctypes.data, vals.ctypes.data, cap,
+                                        ctypes.byref(tn)), "cuapss_build_index")
+        return dim_ptr, rows[:tn.value], vals[:tn.value]
+
+    def feature_remap(self, x: Csr):
+        d, keep = _desc(x)
+        perm = np.empty(x.d, np.int32)
+        counts = np.empty(x.d, np.int32)
+        _check(lib().cuapss_feature_remap(self._h, ctypes.byref(d), perm.ctypes.data,
+                                          counts.ctypes.data), "cuapss_feature_remap")
+        return perm, counts

@@ -1,0 +1,373 @@
+#!/usr/bin/env python3
+"""All-pairs cosine similarity search benchmark (pairs/s).
+
+Workload (default): the plain hybrid APSS at scale -- n = 800,000 vectors,
+d = 50,000, nnz/row lognormal(mean 75, sigma 1.0) clipped at 3,000, Zipf(1.1)
+feature ids, tf-log values, 2% planted near-duplicates, threshold t = 0.7,
+seeded synthetic data (the reference's corpus is not distributed).
+
+A step is one complete self-join of that matrix: validate, frequency remap,
+row order, head block and inverted lists, all 128 x 128 pair tiles, the exact
+finalize and the sorted (i, j, sim) list. value = n(n-1)/2 pairs per step x
+steps x ranks / device time (inputs already in HBM). e2e is the same metric
+through the C ABI with pinned host buffers: the CSR upload and the pair-list
+download are inside the timed region.
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+Multi-GPU (torchrun): every rank runs its own replica of the workload (the
+path has no cross-GPU exchange); value sums the ranks, time is the max.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+for _p in (ROOT, os.path.join(ROOT, "apss-cuda_b200")):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+METRIC = "APSS pairs/s (all-pairs throughput n(n-1)/2 / time, exact pair set vs FP64 oracle)"
+WORKLOAD = "plain_800k"
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            m = json.load(f)
+        return float(m["hbm_gbs"]), float(m["bf16_tflops"]), "measured"
+    except Exception:
+        return 6650.0, 1590.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampler run during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+        return self
+
+    def __exit__(self, *a):
+        if self.p is not None:
+            self.p.terminate()
+            try:
+                self.p.wait(timeout=5)
+            except Exception:
+                self.p.kill()
+
+    def summary(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.f.flush()
+        rows = []
+        with open(self.f.name) as fh:
+            for ln in fh:
+                parts = [x.strip() for x in ln.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.f.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = sorted(float(r[1]) for r in rows if r[1].replace(".", "").isdigit())
+        mx = max((float(r[2]) for r in rows if r[2].replace(".", "").isdigit()), default=None)
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k] == "Active"})
+        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": mx,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def cpu_baseline(x, t, p, budget_s=12.0):
+    """OpenMP FP32 hybrid (oracle/oracle.c cpu_hybrid_apss) on a bounded
+    sample of query rows of the same workload; extrapolated to the full job."""
+    from oracle import oracle
+    threads = oracle.max_threads()
+    q = 32
+    _, prep, qs = oracle.cpu_hybrid(x, t, p, 0, q, threads)
+    per_row = max(qs / q, 1e-6)
+    q = int(min(x.n, max(q, budget_s / per_row)))
+    _, prep, qs = oracle.cpu_hybrid(x, t, p, 0, q, threads)
+    covered = q * (x.n - 1) - q * (q - 1) / 2
+    total = x.n * (x.n - 1) / 2
+    full_time = prep + qs * total / covered
+    return {"value": total / full_time, "unit": "pairs/s", "cores": threads, "kind": "port",
+            "sample": f"query rows 0..{q} of the workload against all j > i "
+                      f"({covered:.3g} of {total:.3g} pairs, {qs:.1f} s) + full preprocessing "
+                      f"({prep:.1f} s), extrapolated to the whole self-join"}
+
+
+def run_reference(args, rank, world):
+    """--impl reference: the reference's own CPU search (InvertedIndex_search,
+    main.cu:104-141, built from its source into oracle/_ref/) on bounded
+    samples of the workload, one process per host core group."""
+    if rank != 0:
+        return
+    from cuapss import synth
+    from oracle import oracle
+    exe = oracle.ref_cpu_search_path()
+    x = synth.generate(WORKLOAD, n=args.n) if args.n else synth.generate(WORKLOAD)
+    total_pairs = x.n * (x.n - 1) / 2
+    if exe is None:
+        # no reference build here: time the CPU port instead
+        vals = []
+        for _ in range(args.warmup + args.steps):
+            vals.append(cpu_baseline(x, args.t, 64, budget_s=8.0))
+        v = vals[-args.steps:]
+        value = sum(b["value"] for b in v) / len(v)
+        line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "pairs/s",
+                "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                "higher_is_better": True, "config": {"workload": WORKLOAD, "n": x.n, "t": args.t},
+                "cpu_baseline": dict(v[-1], value=value),
+                "e2e": {"value": value, "unit": "pairs/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return
+    nproc = max(1, min(os.cpu_count() or 1, 32))
+    n_e = min(x.n, args.ref_index_rows)
+    e = x.rows(0, n_e)
+    td = tempfile.mkdtemp()
+    pe = os.path.join(td, "e.csr")
+    e.save(pe)
+
+    def one_step(q_per_proc):
+        procs, files = [], []
+        for k in range(nproc):
+            lo = n_e + k * q_per_proc
+            if lo + q_per_proc > x.n:
+                lo = (k * q_per_proc) % max(1, x.n - q_per_proc)
+            b = x.rows(lo, lo + q_per_proc)
+            pb = os.path.join(td, f"b{k}.csr")
+            b.save(pb)
+            files.append(pb)
+            procs.append(subprocess.Popen([exe, pb, pe], stdout=subprocess.PIPE,
+                                          stderr=subprocess.DEVNULL, text=True))
+        secs = []
+        for pr in procs:
+            out, _ = pr.communicate()
+            for ln in out.splitlines():
+                if ln.startswith("search_seconds="):
+                    secs.append(float(ln.split("=")[1]))
+        if len(secs) != nproc:
+            raise RuntimeError("reference harness failed")
+        return max(secs)
+
+    # calibrate: seconds per query row
+    t1 = one_step(2)
+    q = max(2, int(args.ref_step_s / max(t1 / 2, 1e-3)))
+    for _ in range(args.warmup):
+        one_step(q)
+    times = [one_step(q) for _ in range(args.steps)]
+    secs = sum(times) / len(times)
+    ordered = nproc * q * n_e
+    value = 0.5 * ordered / secs  # unordered-pair rate of a self-join by this method
+    sample = (f"{nproc} processes x {q} query rows against the reference's inverted index of "
+              f"{n_e} rows ({ordered:.3g} ordered pairs per step, {secs:.1f} s); a self-join "
+              f"visits each unordered pair twice, so value = ordered rate / 2")
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "pairs/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": secs * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "n": x.n, "d": x.d, "t": 0.8,
+                       "note": "the reference's CPU search has t = 0.8 hard-coded"},
+            "cpu_baseline": {"value": value, "unit": "pairs/s", "cores": nproc,
+                             "kind": "reference", "sample": sample},
+            "e2e": {"value": value, "unit": "pairs/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="cuapss", choices=["cuapss", "reference"])
+    ap.add_argument("--t", type=float, default=0.7)
+    ap.add_argument("--n", type=int, default=0, help="override n (smaller quick runs)")
+    ap.add_argument("--head", type=int, default=0, help="head width p (0: library default)")
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "mixed"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--ref-index-rows", type=int, default=100_000)
+    ap.add_argument("--ref-step-s", type=float, default=8.0)
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+
+    import numpy as np
+    import torch
+
+    import cuapss
+    from cuapss import synth
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    x = synth.generate(WORKLOAD, n=args.n) if args.n else synth.generate(WORKLOAD)
+    prec = cuapss.PREC_MIXED if args.precision == "mixed" else cuapss.PREC_FP32
+    dev = {"rowptr": torch.from_numpy(x.rowptr).cuda(), "col": torch.from_numpy(x.col).cuda(),
+           "val": torch.from_numpy(x.val).cuda(), "d": x.d}
+    stream = torch.cuda.Stream()
+    ctx = cuapss.Context(device=local, precision=prec, head_width=args.head,
+                         stream=stream.cuda_stream)
+    cap = 1 << 22
+    out = None
+
+    def alloc(c):
+        return {"i": torch.empty(c, dtype=torch.int32, device="cuda"),
+                "j": torch.empty(c, dtype=torch.int32, device="cuda"),
+                "sim": torch.empty(c, dtype=torch.float32, device="cuda")}
+
+    out = alloc(cap)
+
+    def step():
+        nonlocal out, cap
+        while True:
+            try:
+                return ctx.run_device(dev, args.t, out)
+            except cuapss.CuapssError as e:
+                if e.status != cuapss.EOVERFLOW:
+                    raise
+                cap = ctx.required + 1024
+                out = alloc(cap)
+
+    for _ in range(max(args.warmup, 1)):
+        npairs = step()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    stats = []
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with Clocks(local) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            npairs = step()
+            stats.append(dict(ctx.last_stats))
+        e1.record(stream)
+        torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    ms = e0.elapsed_time(e1) / args.steps
+    if dist:
+        tms = torch.tensor([ms], device="cuda")
+        dist.all_reduce(tms, op=dist.ReduceOp.MAX)
+        ms = float(tms.item())
+    pairs_per_step = x.n * (x.n - 1) / 2
+    value = world * pairs_per_step / (ms / 1e3)
+    clocks = clk.summary()
+
+    # ---- end to end through the C ABI with pinned host buffers ----
+    e2e = None
+    if not args.no_e2e:
+        hp = {"rowptr": torch.from_numpy(x.rowptr).pin_memory(),
+              "col": torch.from_numpy(x.col).pin_memory(),
+              "val": torch.from_numpy(x.val).pin_memory()}
+        hcap = max(npairs, 1)
+        ho = {"i": torch.empty(hcap, dtype=torch.int32).pin_memory(),
+              "j": torch.empty(hcap, dtype=torch.int32).pin_memory(),
+              "sim": torch.empty(hcap, dtype=torch.float32).pin_memory()}
+        desc = cuapss.CsrDesc(x.n, x.d, x.nnz, hp["rowptr"].data_ptr(), hp["col"].data_ptr(),
+                              hp["val"].data_ptr(), 0)
+        L = cuapss.lib()
+
+        def hstep():
+            pr = cuapss.PairsDesc(ho["i"].data_ptr(), ho["j"].data_ptr(), ho["sim"].data_ptr(),
+                                  hcap, 0, 0)
+            s = L.cuapss_run(ctx._h, ctypes.byref(desc), ctypes.c_float(args.t),
+                             ctypes.byref(pr), None)
+            if s != cuapss.OK:
+                raise cuapss.CuapssError(s, "cuapss_run (host buffers)")
+            return int(pr.count)
+
+        hstep()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        f0 = torch.cuda.Event(enable_timing=True)
+        f1 = torch.cuda.Event(enable_timing=True)
+        f0.record(stream)
+        for _ in range(args.steps):
+            hn = hstep()
+        f1.record(stream)
+        torch.cuda.synchronize()
+        ems = f0.elapsed_time(f1) / args.steps
+        if dist:
+            tms = torch.tensor([ems], device="cuda")
+            dist.all_reduce(tms, op=dist.ReduceOp.MAX)
+            ems = float(tms.item())
+        e2e = {"value": world * pairs_per_step / (ems / 1e3), "unit": "pairs/s",
+               "ms_per_step": ems,
+               "h2d_bytes_per_step": int(x.rowptr.nbytes + x.col.nbytes + x.val.nbytes),
+               "d2h_bytes_per_step": int(hn * 12)}
+
+    # ---- roofline of the dominant kernel (the pair-tile kernel) ----
+    hbm, bf16, src = peaks()
+    tile_ms = sum(s["ms_tiles"] for s in stats) / len(stats)
+    s0 = stats[-1]
+    p = int(s0["head_width"])
+    alg_bytes = 8.0 * s0["tail_products"] + 4.0 * p * x.n + 12.0 * s0["candidates"]
+    achieved_gbs = alg_bytes / (tile_ms / 1e3) / 1e9
+    fma_tflops = 2.0 * p * pairs_per_step / (tile_ms / 1e3) / 1e12
+    roofline = {"bound": "hbm", "achieved": achieved_gbs, "peak": hbm, "unit": "GB/s",
+                "frac": achieved_gbs / hbm, "traffic": None, "peak_source": src,
+                "kernel": "k_tiles_fp32", "kernel_ms": tile_ms,
+                "algorithmic_bytes": alg_bytes,
+                "note": "FP32 head runs on CUDA cores (FMA-bound); head FP32 FMA rate "
+                        f"{fma_tflops:.1f} TFLOP/s"}
+    line = {
+        "metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32" if prec == cuapss.PREC_FP32 else "bf16+f32",
+        "data": "synthetic (seeded generator, reference corpus not distributed)",
+        "config": {"workload": WORKLOAD, "n": x.n, "d": x.d, "nnz": x.nnz, "t": args.t,
+                   "precision": args.precision, "head_width": p,
+                   "l2": "inputs larger than L2 (CSR + head block > 126 MB)",
+                   "parallelism": f"replicas x{world}"},
+        "pairs_found": npairs, "candidates": s0["candidates"], "rescored": s0["rescored"],
+        "stage_ms": {k: sum(s[k] for s in stats) / len(stats)
+                     for k in ("ms_preprocess", "ms_tiles", "ms_finalize", "ms_total")},
+        "gpu_launches": int(sum(s["launches"] for s in stats)),
+        "clocks": clocks, "roofline": roofline, "e2e": e2e,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu:
+        line["cpu_baseline"] = cpu_baseline(x, args.t, p)
+    if rank == 0:
+        print(json.dumps(line))
+    ctx.close()
+    if dist:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,171 @@
+/*
+ * cuapss.h -- C ABI of the B200-native hybrid all-pairs cosine similarity
+ * search (APSS).
+ *
+ * Input : a CSR matrix of L2-normalised sparse vectors (n rows, d features,
+ *         int64 row pointers, int32 feature ids sorted ascending in each row,
+ *         float32 values) and a threshold t.
+ * Output: every unordered pair (i, j), i < j, whose cosine similarity
+ *         (= dot product of the normalised rows) is >= t, with its similarity.
+ *
+ * This replaces the single entry point of the reference,
+ *   void similarity_join_device(int* dim_A, float* feature_A, int* tile_start_A,
+ *                               ... x8 partitions ..., int* b_id_a,
+ *                               int* apss_block_seg, int* apss_seg_start)
+ * (similarity_search.h:3-14, defined similarity_search.cu:934-3014), which
+ * takes a tile-ELL layout of 8 fixed partitions, allocates its own device
+ * memory, returns void and only prints pair counts. The reference's
+ * signature itself is kept as a compatibility shim, cuapss_compat.h.
+ *
+ * Conventions
+ *  - Every call returns a cuapss_status. Nothing is printed.
+ *  - A context owns one CUDA stream (its own or the caller's) and is used by
+ *    one host thread at a time.
+ *  - Pointers flagged on_device are CUDA device pointers on the context's
+ *    device; otherwise they are host pointers (pinned or pageable).
+ *  - Pair output is sorted by (i, j) ascending, i < j, in the caller's row
+ *    numbering. If the caller's capacity is too small the call returns
+ *    CUAPSS_EOVERFLOW with pairs->count set to the required capacity; the
+ *    caller retries with a larger buffer (the search is deterministic).
+ *  - Exactness contract: the emitted pair set equals the set of pairs whose
+ *    similarity, accumulated in FP64 from the FP32 inputs in ascending
+ *    feature-id order, is >= t. Each reported similarity is within 1e-6 of
+ *    that FP64 value.
+ */
+#ifndef CUAPSS_H_
+#define CUAPSS_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CUAPSS_ABI_VERSION 1
+
+typedef enum {
+  CUAPSS_OK = 0,
+  CUAPSS_EINVAL = 1,    /* malformed CSR, bad option, not normalised, bad t */
+  CUAPSS_ENOMEM = 2,    /* device or host allocation failed */
+  CUAPSS_EOVERFLOW = 3, /* output capacity too small; count = required */
+  CUAPSS_ETIMEOUT = 4,  /* a bounded wait gave up (serving loop) */
+  CUAPSS_ECUDA = 5,     /* a CUDA runtime call failed */
+  CUAPSS_EBUSY = 6      /* admission refused: HBM budget or queue full */
+} cuapss_status;
+
+typedef enum {
+  CUAPSS_PREC_FP32 = 0,  /* plain FP32 hybrid: head on the forward-list dot */
+  CUAPSS_PREC_MIXED = 1  /* BF16 head on tcgen05, FP32 tail, FP64 rescore  */
+} cuapss_precision;
+
+typedef struct {
+  int device;          /* CUDA device ordinal */
+  void* stream;        /* cudaStream_t to launch on; NULL: context creates one */
+  int precision;       /* cuapss_precision */
+  int head_width;      /* p, the number of most frequent features handled by
+                          the pair-parallel head; 0 = autotuner picks */
+  int remap;           /* 1 (default): frequency-ordered feature remap;
+                          0: identity, head = feature ids < p (reference rule) */
+  int validate;        /* 1 (default): check CSR structure and row norms */
+  float norm_tol;      /* accepted | ||x||_2 - 1 | (default 1e-4) */
+  int verbose;         /* reserved, 0 */
+} cuapss_opts;
+
+typedef struct {
+  int64_t n;              /* rows (vectors) */
+  int64_t d;              /* features (dimension) */
+  int64_t nnz;            /* non-zeros */
+  const int64_t* rowptr;  /* [n+1] */
+  const int32_t* col;     /* [nnz] feature ids, strictly ascending per row */
+  const float* val;       /* [nnz] */
+  int on_device;          /* 1: the three arrays are device pointers */
+} cuapss_csr;
+
+typedef struct {
+  int32_t* i;        /* [capacity] first row id  (i < j) */
+  int32_t* j;        /* [capacity] second row id */
+  float* sim;        /* [capacity] similarity */
+  int64_t capacity;  /* entries available in i, j, sim */
+  int64_t count;     /* out: pairs found (required capacity on EOVERFLOW) */
+  int on_device;     /* 1: i, j, sim are device pointers */
+} cuapss_pairs;
+
+typedef struct {
+  int64_t pairs;          /* pairs emitted (sim >= t) */
+  int64_t candidates;     /* pairs that left the tile epilogue */
+  int64_t rescored;       /* candidates inside the error band, redone in FP64 */
+  int64_t tiles;          /* 128x128 pair tiles evaluated */
+  int64_t head_width;     /* p used */
+  int64_t tail_entries;   /* non-zeros outside the head */
+  int64_t tail_products;  /* sum over tail features of L(L-1)/2 */
+  double max_band;        /* largest error margin used by the epilogue */
+  double ms_preprocess;   /* validate + remap + row order + norms + layout */
+  double ms_index;        /* inverted lists (block-local and global) */
+  double ms_tiles;        /* head dot + tail scan + epilogue */
+  double ms_finalize;     /* rescore, compensated re-score, sort, copy-out */
+  double ms_total;
+  int64_t launches;       /* CUDA kernels this call launched */
+} cuapss_stats;
+
+typedef struct cuapss_ctx cuapss_ctx;
+
+/* Defaults for cuapss_opts (device 0, own stream, FP32, autotuned p, remap,
+ * validation on, norm_tol 1e-4). */
+void cuapss_default_opts(cuapss_opts* opts);
+
+/* Human-readable name of a status code. */
+const char* cuapss_status_string(cuapss_status s);
+
+/* Runtime ABI version (CUAPSS_ABI_VERSION of the built library). */
+int cuapss_abi_version(void);
+
+/* Create / destroy a context. Replaces the allocation prologue and the
+ * (partial) frees of similarity_join_device (similarity_search.cu:946-1075,
+ * 2996-3013). */
+cuapss_status cuapss_create(cuapss_ctx** ctx, const cuapss_opts* opts);
+cuapss_status cuapss_destroy(cuapss_ctx* ctx);
+
+/* Self-join: all pairs i < j of `x` with sim >= t. Replaces the eight
+ * intra-partition "apss" pipelines of similarity_join_device
+ * (similarity_search.cu:2650-2993) and, since the whole input is one matrix,
+ * also the 28 cross-partition joins (similarity_search.cu:1273-2632).
+ * `stats` may be NULL. Synchronous: returns when `out` is filled. */
+cuapss_status cuapss_run(cuapss_ctx* ctx, const cuapss_csr* x, float t,
+                         cuapss_pairs* out, cuapss_stats* stats);
+
+/* Cross-join: all pairs (a, b), a row of `a`, b row of `b`, sim >= t.
+ * out->i holds the row of `a`, out->j the row of `b`; sorted by (i, j).
+ * This is the per-partition-pair join of the reference
+ * (similarity_join1 / filter_pair / similarity_join_rest,
+ * similarity_search.cu:370-531, launched at 1273-2632). */
+cuapss_status cuapss_join(cuapss_ctx* ctx, const cuapss_csr* a,
+                          const cuapss_csr* b, float t, cuapss_pairs* out,
+                          cuapss_stats* stats);
+
+/* Inverted index of the tail features, reference semantics: for every
+ * feature f with f >= p (on the caller's ids, no remap), the rows that
+ * contain f and their values, lists sorted by row. dim_ptr has d+1 entries
+ * (exclusive scan of the per-feature counts; features < p have empty lists).
+ * Replaces generate_index_ptr4 + the host scan + construct_Index2
+ * (similarity_search.cu:105-191, 1168-1186, 221-274), whose list order is
+ * nondeterministic; sorted by row the two are equal. All arrays are device
+ * pointers if x->on_device, else host. idx_row/idx_val need capacity
+ * >= number of tail non-zeros (returned in *tail_nnz; EOVERFLOW if short). */
+cuapss_status cuapss_build_index(cuapss_ctx* ctx, const cuapss_csr* x,
+                                 int32_t p, int32_t* dim_ptr, int32_t* idx_row,
+                                 float* idx_val, int64_t capacity,
+                                 int64_t* tail_nnz);
+
+/* Frequency-ordered feature remap: perm[f] = rank of feature f when features
+ * are sorted by (posting count descending, id ascending); counts[f] = the
+ * posting count. Device pointers if x->on_device. (No counterpart in the
+ * reference, which fixes the head to ids < 4096.) */
+cuapss_status cuapss_feature_remap(cuapss_ctx* ctx, const cuapss_csr* x,
+                                   int32_t* perm, int32_t* counts);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CUAPSS_H_ */
