@@ -16,6 +16,7 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <vector>
 
 #include "ctx.cuh"
 #include "index.cuh"
@@ -144,7 +145,6 @@ cuapss_status join_device(cuapss_ctx* ctx, const DevCsr& a, const DevCsr* b, flo
     SB.nnz = bb.nnz;
     SB.nrm_max = nrm_b;
     ST_TRY(build_side(SB, po, perm, ws, "B", st));
-    ST_TRY(link_tail(SA, SB, false, st));
     SJ = &SB;
   }
   cudaEventRecord(ctx->ev[1], st);
@@ -155,26 +155,54 @@ cuapss_status join_device(cuapss_ctx* ctx, const DevCsr& a, const DevCsr* b, flo
   ta.headI32 = SA.head32;
   ta.nI = SA.n;
   ta.nbI = SA.nb;
-  ta.tptrI = SA.tptr;
-  ta.tcur0 = SA.tcur0;
-  ta.tend = SA.tend;
-  ta.tr = SA.tr;
-  ta.tu = SA.tu;
   ta.blkmaxI = SA.blk_maxnnz;
   ta.hnormI = SA.hnorm;
+  ta.gptrI = SA.gptr;
+  ta.gstartI = SA.gstart;
+  ta.gfeatI = SA.gfeat;
+  ta.bilI_f = SA.bil_f;
+  ta.bilI_r = SA.bil_r;
+  ta.bilI_u = SA.bil_u;
   ta.headJ32 = SJ->head32;
   ta.nJ = SJ->n;
   ta.nbJ = SJ->nb;
-  ta.cscJ = SJ->csc;
   ta.blkmaxJ = SJ->blk_maxnnz;
   ta.hnormJ = SJ->hnorm;
+  ta.bptrJ = SJ->bptr;
+  ta.bilJ_rec = SJ->bil_rec;
   ta.p = SA.p;
   ta.self = self ? 1 : 0;
   ta.t = t;
-  ta.eps_c1 = u * nrm2 * 1.001;
-  ta.eps_c0 = 2.0 * u * nrm2 * 1.001 + 1e-10;
+  // FP32 head chain + fixed-point tail (2^-30 grid, exact sums) + final add:
+  // |s~ - s| <= (K + 3) u ||a|| ||b|| + K 2^-31, K = shared features
+  if (nrm2 >= 1.9) return CUAPSS_EINVAL;  // fixed-point tail needs ~unit norms
+  ta.eps_c1 = (u * nrm2 + std::ldexp(1.0, -31)) * 1.001;
+  ta.eps_c0 = 3.0 * u * nrm2 * 1.001 + 1e-10;
   ta.eps_head = 0.0;
-  ta.nunits = self ? (int)((SA.nb + 1) / 2) : SA.nb;
+  // ---- units: I block x J range, heavy I blocks cut into short ranges ----
+  const int grid_max = ctx->sms;
+  std::vector<int4> units;
+  {
+    const double avg = std::max(1.0, (double)SA.ntail / std::max(1, SA.nb));
+    auto weight = [&](int I) {
+      return 1.0 + (double)(SA.h_bptr[I + 1] - SA.h_bptr[I]) / avg;
+    };
+    double total = 0.0;
+    for (int I = 0; I < SA.nb; ++I) total += weight(I) * (SJ->nb - (self ? I : 0));
+    const double target = std::max(1.0, total / (grid_max * 16.0));
+    for (int I = 0; I < SA.nb; ++I) {
+      const int jb = self ? I : 0, je = SJ->nb;
+      const int chunk = (int)std::max(1.0, std::floor(target / weight(I)));
+      for (int j0 = jb; j0 < je; j0 += chunk) units.push_back(make_int4(I, j0, std::min(je, j0 + chunk), 0));
+    }
+  }
+  int4* d_units = nullptr;
+  ST_TRY(ws.get("tiles:units", std::max<size_t>(units.size(), 1), &d_units));
+  if (!units.empty())
+    CU_TRY(cudaMemcpyAsync(d_units, units.data(), sizeof(int4) * units.size(),
+                           cudaMemcpyHostToDevice, st));
+  ta.units = d_units;
+  ta.nunits = (int)units.size();
   int64_t ncand = 0;
   int* unit_counter = nullptr;
   int* err = nullptr;
@@ -182,11 +210,7 @@ cuapss_status join_device(cuapss_ctx* ctx, const DevCsr& a, const DevCsr* b, flo
   ST_TRY(ws.get("tiles:unit", 1, &unit_counter));
   ST_TRY(ws.get("tiles:err", 1, &err));
   ST_TRY(ws.get("tiles:ccount", 1, &ccount));
-  const int grid = std::max(1, std::min(ta.nunits, ctx->sms));
-  const int64_t stride = std::max<int64_t>(SA.max_block_tail, 1);
-  ST_TRY(ws.get("tiles:scr_cur", (size_t)grid * stride, &ta.scr_cur));
-  ST_TRY(ws.get("tiles:scr_next", (size_t)grid * stride, &ta.scr_next));
-  ta.scr_stride = stride;
+  const int grid = std::max(1, std::min(ta.nunits, grid_max));
   ta.unit_counter = unit_counter;
   ta.err = err;
   ta.cand_count = ccount;

@@ -204,28 +204,79 @@ __global__ void k_head32_scatter(const int64_t* __restrict__ rp2, const int32_t*
   }
 }
 
-// One warp per new row: tail entries in row order + (feature, row) sort keys.
+// One warp per new row: tail entries in row order, sort keys for the
+// block-local lists (block, feature) and, optionally, the global lists
+// (feature, row); posting counts per tail feature.
 __global__ void k_tail_entries(const int64_t* __restrict__ rp2, const int32_t* __restrict__ col2,
                                const float* __restrict__ val2, const int32_t* __restrict__ hlen,
                                const int64_t* __restrict__ tptr, int64_t n, int p, int rbits,
-                               uint32_t* __restrict__ tk, uint8_t* __restrict__ tr,
-                               float* __restrict__ tu, uint64_t* __restrict__ keys,
-                               uint32_t* __restrict__ vals, int32_t* __restrict__ ccount) {
+                               int fb, uint32_t* __restrict__ tk, uint8_t* __restrict__ tr,
+                               float* __restrict__ tu, uint64_t* __restrict__ ckeys,
+                               uint32_t* __restrict__ cvals, uint64_t* __restrict__ bkeys,
+                               uint32_t* __restrict__ bvals, int32_t* __restrict__ ccount) {
   const int lane = threadIdx.x & 31;
   const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
   for (int64_t r = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; r < n; r += warps) {
     const int64_t lo = rp2[r] + hlen[r], hi = rp2[r + 1];
     const int64_t t0 = tptr[r];
+    const uint64_t blk = (uint64_t)(r / kBlockRows);
     for (int64_t k = lo + lane; k < hi; k += 32) {
       const int64_t t = t0 + (k - lo);
       const int32_t f = col2[k] - p;
       tk[t] = (uint32_t)k;
       tr[t] = (uint8_t)(r % kBlockRows);
       tu[t] = val2[k];
-      keys[t] = ((uint64_t)f << rbits) | (uint64_t)r;
-      vals[t] = (uint32_t)t;
+      bkeys[t] = (blk << fb) | (uint64_t)f;
+      bvals[t] = (uint32_t)t;
+      if (ckeys) {
+        ckeys[t] = ((uint64_t)f << rbits) | (uint64_t)r;
+        cvals[t] = (uint32_t)t;
+      }
       atomicAdd(&ccount[f], 1);
     }
+  }
+}
+
+__global__ void k_bil_fill(const uint64_t* __restrict__ keys, const uint32_t* __restrict__ vals,
+                           const uint8_t* __restrict__ tr, const float* __restrict__ tu, int64_t T,
+                           uint64_t fmask, uint32_t* __restrict__ bil_f, uint8_t* __restrict__ bil_r,
+                           float* __restrict__ bil_u, uint2* __restrict__ bil_rec,
+                           uint32_t* __restrict__ flags) {
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < T;
+       k += (int64_t)gridDim.x * blockDim.x) {
+    const uint64_t key = keys[k];
+    const uint32_t t = vals[k];
+    const uint32_t f = (uint32_t)(key & fmask);
+    bil_f[k] = f;
+    bil_r[k] = tr[t];
+    bil_u[k] = tu[t];
+    bil_rec[k] = make_uint2((f << 8) | (uint32_t)tr[t], __float_as_uint(tu[t]));
+    flags[k] = (k == 0 || keys[k - 1] != key) ? 1u : 0u;
+  }
+}
+
+__global__ void k_group_starts(const uint32_t* __restrict__ flags, const uint32_t* __restrict__ gidx,
+                               const uint32_t* __restrict__ bil_f, int64_t T,
+                               uint32_t* __restrict__ gstart, uint32_t* __restrict__ gfeat) {
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k <= T;
+       k += (int64_t)gridDim.x * blockDim.x) {
+    if (k == T) {
+      gstart[gidx[T]] = (uint32_t)T;
+    } else if (flags[k]) {
+      gstart[gidx[k]] = (uint32_t)k;
+      gfeat[gidx[k]] = bil_f[k];
+    }
+  }
+}
+
+__global__ void k_block_ptrs(const int64_t* __restrict__ tptr, const uint32_t* __restrict__ gidx,
+                             int64_t n, int nb, int64_t* __restrict__ bptr,
+                             int64_t* __restrict__ gptr) {
+  for (int64_t b = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; b <= nb;
+       b += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t e = tptr[min(n, b * kBlockRows)];
+    bptr[b] = e;
+    gptr[b] = gidx[e];
   }
 }
 
@@ -254,38 +305,8 @@ __global__ void k_tail_products(const int32_t* __restrict__ ccount, int64_t nf,
   if ((threadIdx.x & 31) == 0 && s) atomicAdd(out, s);
 }
 
-__global__ void k_block_tail_max(const int64_t* __restrict__ tptr, int64_t n, int nb,
-                                 unsigned long long* out) {
-  for (int64_t b = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; b < nb;
-       b += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t lo = tptr[b * kBlockRows];
-    const int64_t hi = tptr[min(n, (b + 1) * kBlockRows)];
-    atomicMax(out, (unsigned long long)(hi - lo));
-  }
-}
 
-__global__ void k_link_self(const uint32_t* __restrict__ entpos, const uint32_t* __restrict__ tk,
-                            const int32_t* __restrict__ col2, const int64_t* __restrict__ cptr,
-                            int64_t T, int p, uint32_t* __restrict__ tcur0,
-                            uint32_t* __restrict__ tend) {
-  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < T;
-       t += (int64_t)gridDim.x * blockDim.x) {
-    const int32_t f = col2[tk[t]] - p;
-    tcur0[t] = entpos[t] + 1u;
-    tend[t] = (uint32_t)cptr[f + 1];
-  }
-}
 
-__global__ void k_link_cross(const uint32_t* __restrict__ tk, const int32_t* __restrict__ col2,
-                             const int64_t* __restrict__ cptrJ, int64_t T, int p,
-                             uint32_t* __restrict__ tcur0, uint32_t* __restrict__ tend) {
-  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < T;
-       t += (int64_t)gridDim.x * blockDim.x) {
-    const int32_t f = col2[tk[t]] - p;
-    tcur0[t] = (uint32_t)cptrJ[f];
-    tend[t] = (uint32_t)cptrJ[f + 1];
-  }
-}
 
 __global__ void k_widen_i32(const int32_t* __restrict__ a, int64_t* __restrict__ b, int64_t m) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < m;
@@ -419,37 +440,72 @@ cuapss_status build_side(Side& s, const PrepOptions& o, const int32_t* perm, Wor
                                                                       s.hlen, n, p, s.head32);
     LAUNCH_CHECK();
   }
-  // ---- tail: entries in row order and the global inverted lists ----
+  // ---- tail: entries in row order, block-local inverted lists, groups ----
   CU_TRY(cudaMemcpyAsync(&s.ntail, s.tptr + n, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
   CU_TRY(cudaStreamSynchronize(st));
   const int64_t T = s.ntail;
+  if (T >= (int64_t)UINT32_MAX - 1) return CUAPSS_EINVAL;
   const int64_t nf = std::max<int64_t>(d - p, 0);
-  uint64_t* tkeys = nullptr;
-  uint32_t* tvals = nullptr;
+  if (nf >= (1 << 24)) return CUAPSS_EINVAL;  // packed postings hold 24-bit features
+  const int fb = std::max(1, bits_for((uint64_t)nf));
+  const int bb = std::max(1, bits_for((uint64_t)nb));
+  uint64_t *ckeys = nullptr, *bkeys = nullptr;
+  uint32_t *cvals = nullptr, *bvals = nullptr, *flags = nullptr;
   int32_t* ccount = nullptr;
-  uint32_t* entpos = nullptr;
   ST_TRY(ws.get(t + "tk", (size_t)T, &s.tk));
   ST_TRY(ws.get(t + "tr", (size_t)T, &s.tr));
   ST_TRY(ws.get(t + "tu", (size_t)T, &s.tu));
-  ST_TRY(ws.get(t + "tcur0", (size_t)T, &s.tcur0));
-  ST_TRY(ws.get(t + "tend", (size_t)T, &s.tend));
-  ST_TRY(ws.get(t + "tkeys", (size_t)T, &tkeys));
-  ST_TRY(ws.get(t + "tvals", (size_t)T, &tvals));
-  ST_TRY(ws.get(t + "entpos", (size_t)T, &entpos));
+  ST_TRY(ws.get(t + "bkeys", (size_t)T, &bkeys));
+  ST_TRY(ws.get(t + "bvals", (size_t)T, &bvals));
   ST_TRY(ws.get(t + "ccount", (size_t)nf + 1, &ccount));
-  ST_TRY(ws.get(t + "cptr", (size_t)nf + 1, &s.cptr));
-  ST_TRY(ws.get(t + "csc", (size_t)T, &s.csc));
+  if (o.want_csc) {
+    ST_TRY(ws.get(t + "ckeys", (size_t)T, &ckeys));
+    ST_TRY(ws.get(t + "cvals", (size_t)T, &cvals));
+  }
   CU_TRY(cudaMemsetAsync(ccount, 0, sizeof(int32_t) * (nf + 1), st));
   k_tail_entries<<<grid_for(n * 32, kThreads), kThreads, 0, st>>>(
-      s.rp2, s.col2, s.val2, s.hlen, s.tptr, n, p, rbits, s.tk, s.tr, s.tu, tkeys, tvals, ccount);
+      s.rp2, s.col2, s.val2, s.hlen, s.tptr, n, p, rbits, fb, s.tk, s.tr, s.tu, ckeys, cvals,
+      bkeys, bvals, ccount);
   LAUNCH_CHECK();
-  ST_TRY(radix_sort_pairs(tkeys, tvals, T, rbits + std::max(1, bits_for((uint64_t)nf)), ws,
-                          t + "csc", st));
-  k_csc_fill<<<grid_for(T, kThreads), kThreads, 0, st>>>(tkeys, tvals, s.tk, s.val2, T, rmask,
-                                                        s.csc, entpos);
+  // block-local inverted lists: stable sort by (block, feature) keeps rows
+  // ascending inside a feature; groups come from a scan of head flags
+  ST_TRY(radix_sort_pairs(bkeys, bvals, T, bb + fb, ws, t + "bil", st));
+  ST_TRY(ws.get(t + "bil_f", (size_t)T, &s.bil_f));
+  ST_TRY(ws.get(t + "bil_r", (size_t)T, &s.bil_r));
+  ST_TRY(ws.get(t + "bil_u", (size_t)T, &s.bil_u));
+  ST_TRY(ws.get(t + "bil_rec", (size_t)T, &s.bil_rec));
+  ST_TRY(ws.get(t + "gflags", (size_t)T + 1, &flags));
+  k_bil_fill<<<grid_for(T, kThreads), kThreads, 0, st>>>(bkeys, bvals, s.tr, s.tu, T,
+                                                        (1ull << fb) - 1, s.bil_f, s.bil_r,
+                                                        s.bil_u, s.bil_rec, flags);
   LAUNCH_CHECK();
-  {
-    // int32 counts -> int64 list pointers
+  uint32_t* gidx = nullptr;
+  ST_TRY(ws.get(t + "gidx", (size_t)T + 1, &gidx));
+  ST_TRY(exclusive_scan<uint32_t>(flags, gidx, T, gidx + T, ws, t + "gidx", st));
+  uint32_t G32 = 0;
+  CU_TRY(cudaMemcpyAsync(&G32, gidx + T, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+  CU_TRY(cudaStreamSynchronize(st));
+  s.ngroups = G32;
+  ST_TRY(ws.get(t + "gstart", (size_t)s.ngroups + 1, &s.gstart));
+  ST_TRY(ws.get(t + "gfeat", (size_t)s.ngroups + 1, &s.gfeat));
+  ST_TRY(ws.get(t + "bptr", (size_t)nb + 1, &s.bptr));
+  ST_TRY(ws.get(t + "gptr", (size_t)nb + 1, &s.gptr));
+  k_group_starts<<<grid_for(T + 1, kThreads), kThreads, 0, st>>>(flags, gidx, s.bil_f, T,
+                                                                   s.gstart, s.gfeat);
+  LAUNCH_CHECK();
+  k_block_ptrs<<<grid_for(nb + 1, kThreads), kThreads, 0, st>>>(s.tptr, gidx, n, nb, s.bptr,
+                                                                 s.gptr);
+  LAUNCH_CHECK();
+  // ---- global inverted lists (feature, row), on request ----
+  if (o.want_csc) {
+    uint32_t* entpos = nullptr;
+    ST_TRY(ws.get(t + "entpos", (size_t)T, &entpos));
+    ST_TRY(ws.get(t + "cptr", (size_t)nf + 1, &s.cptr));
+    ST_TRY(ws.get(t + "csc", (size_t)T, &s.csc));
+    ST_TRY(radix_sort_pairs(ckeys, cvals, T, rbits + fb, ws, t + "csc", st));
+    k_csc_fill<<<grid_for(T, kThreads), kThreads, 0, st>>>(ckeys, cvals, s.tk, s.val2, T, rmask,
+                                                          s.csc, entpos);
+    LAUNCH_CHECK();
     int64_t* c64 = nullptr;
     ST_TRY(ws.get(t + "ccount64", (size_t)nf + 1, &c64));
     k_widen_i32<<<grid_for(nf, kThreads), kThreads, 0, st>>>(ccount, c64, nf);
@@ -461,25 +517,22 @@ cuapss_status build_side(Side& s, const PrepOptions& o, const int32_t* perm, Wor
   CU_TRY(cudaMemsetAsync(red, 0, 2 * sizeof(unsigned long long), st));
   k_tail_products<<<grid_for(nf, kThreads), kThreads, 0, st>>>(ccount, nf, red);
   LAUNCH_CHECK();
-  k_block_tail_max<<<grid_for(nb, kThreads), kThreads, 0, st>>>(s.tptr, n, nb, red + 1);
-  LAUNCH_CHECK();
-  k_link_self<<<grid_for(T, kThreads), kThreads, 0, st>>>(entpos, s.tk, s.col2, s.cptr, T, p,
-                                                         s.tcur0, s.tend);
-  LAUNCH_CHECK();
   unsigned long long hred[2] = {0, 0};
   CU_TRY(cudaMemcpyAsync(hred, red, sizeof(hred), cudaMemcpyDeviceToHost, st));
+  s.h_bptr.resize(nb + 1);
+  s.h_gptr.resize(nb + 1);
+  CU_TRY(cudaMemcpyAsync(s.h_bptr.data(), s.bptr, sizeof(int64_t) * (nb + 1),
+                         cudaMemcpyDeviceToHost, st));
+  CU_TRY(cudaMemcpyAsync(s.h_gptr.data(), s.gptr, sizeof(int64_t) * (nb + 1),
+                         cudaMemcpyDeviceToHost, st));
   CU_TRY(cudaStreamSynchronize(st));
   s.tail_products = (int64_t)hred[0];
-  s.max_block_tail = (int64_t)hred[1];
-  return CUAPSS_OK;
-}
-
-cuapss_status link_tail(Side& I, const Side& J, bool self, cudaStream_t st) {
-  if (self) return CUAPSS_OK;  // build_side already linked a side to itself
-  if (I.p != J.p || I.d != J.d) return CUAPSS_EINVAL;
-  k_link_cross<<<grid_for(I.ntail, kThreads), kThreads, 0, st>>>(I.tk, I.col2, J.cptr, I.ntail,
-                                                                 I.p, I.tcur0, I.tend);
-  LAUNCH_CHECK();
+  s.max_block_tail = 0;
+  s.max_block_groups = 0;
+  for (int b = 0; b < nb; ++b) {
+    s.max_block_tail = std::max<int64_t>(s.max_block_tail, s.h_bptr[b + 1] - s.h_bptr[b]);
+    s.max_block_groups = std::max<int64_t>(s.max_block_groups, s.h_gptr[b + 1] - s.h_gptr[b]);
+  }
   return CUAPSS_OK;
 }
 

@@ -14,6 +14,7 @@ struct PrepOptions {
   int row_sort = 1;     // order rows by nnz descending
   int want_head32 = 1;  // build the FP32 head block
   int want_head16 = 0;  // build the BF16 head block
+  int want_csc = 0;     // build the global inverted lists (cptr/csc)
 };
 
 // Validates a device CSR. counts (device, d entries, may be null) are
@@ -31,9 +32,5 @@ cuapss_status feature_perm(const int32_t* counts, int64_t d, int64_t max_count, 
 cuapss_status build_side(Side& s, const PrepOptions& o, const int32_t* perm, Workspace& ws,
                          const std::string& tag, cudaStream_t st);
 
-// Points the tail cursors of `I` at the inverted lists of `J` (same remap and
-// p). self: I and J are the same side and each entry starts after its own
-// posting, so only pairs i < j are visited.
-cuapss_status link_tail(Side& I, const Side& J, bool self, cudaStream_t st);
 
 }  // namespace cuapss

@@ -15,16 +15,23 @@
 //   head16    bf16            dense head block for the tensor-core path
 //   cptr/csc  int64[d-p+1], {int32 row, f32 val}[T]
 //                             inverted lists of the tail features (rank >= p),
-//                             rows ascending: the global index
+//                             rows ascending: the global index (built on
+//                             request)
 //   tptr      int64[n+1]      tail entries of each row, in row order
-//   tcur0/tend/tr/tu          per tail entry: first posting to visit in the
-//                             J-side index, end of that list, row inside its
-//                             block, value
+//   bptr      int64[nb+1]     tail entries of each row block
+//   bil_f/bil_r/bil_u         block-local inverted lists: the tail postings
+//                             of each row block sorted by (feature, row):
+//                             feature - p, row inside the block, value
+//   gstart    uint32[G+1]     feature groups: entries [gstart[g], gstart[g+1])
+//                             of the BIL share one feature
+//   gfeat     uint32[G]       feature of each group
+//   gptr      int64[nb+1]     groups of each row block
 #pragma once
 
 #include <cuda_bf16.h>
 
 #include <cstdint>
+#include <vector>
 
 #include "common.cuh"
 
@@ -52,12 +59,22 @@ struct Side {
   uint32_t* tk = nullptr;         // tail entry -> index into col2/val2
   int64_t* cptr = nullptr;
   uint2* csc = nullptr;
-  uint32_t* tcur0 = nullptr;
-  uint32_t* tend = nullptr;
-  uint8_t* tr = nullptr;
+  uint8_t* tr = nullptr;          // row-order tail entries: row in block, value
   float* tu = nullptr;
+  int64_t* bptr = nullptr;
+  uint32_t* bil_f = nullptr;
+  uint8_t* bil_r = nullptr;
+  float* bil_u = nullptr;
+  uint2* bil_rec = nullptr;       // packed posting {feature << 8 | row, value bits}
+  uint32_t* gstart = nullptr;
+  uint32_t* gfeat = nullptr;      // feature of each group
+  int64_t* gptr = nullptr;
+  int64_t ngroups = 0;
+  int64_t max_block_groups = 0;
   int64_t ntail = 0;
   int64_t max_block_tail = 0;
+  std::vector<int64_t> h_bptr;    // host copy of bptr (unit scheduling)
+  std::vector<int64_t> h_gptr;    // host copy of gptr
   int64_t tail_products = 0;      // sum over tail lists of L(L-1)/2
   double nrm_max = 1.0;           // largest row norm (FP64)
 };

@@ -2,11 +2,10 @@
 //
 // One CTA evaluates 128 x 128 pair tiles (I block of rows x J block of
 // columns) of the similarity matrix:
-//  1. tail, feature-parallel: every tail posting (row r of I, feature f,
-//     value u) keeps a cursor into the inverted list of f in the J-side
-//     index; postings of f whose row falls in J are consumed and
-//     u * v is added into a shared-memory accumulator acc[r][c] with
-//     shared-memory atomics (the role of similarity_apss1 /
+//  1. tail, feature-parallel (tail.cuh): the J block's block-local inverted
+//     list is merged against the I block's feature groups (staged in shared
+//     memory) and every common feature adds u * v into a shared-memory
+//     accumulator acc[r][c] with shared-memory atomics (the role of similarity_apss1 /
 //     similarity_join1, fengyilin118/APSS-CUDA similarity_search.cu:370-437
 //     and 642-735, which instead add into a dense n x n global array);
 //  2. head, pair-parallel: the dense head blocks of I and J (p features, 32
@@ -21,12 +20,14 @@
 //     pairs at exactly t); surviving pairs are compacted with a warp ballot
 //     and one atomic per warp into the candidate list (the reference counts
 //     nothing: its atomicAdd(sum_pair) is commented out, 501 and 910).
-// Units of work are taken from a global counter (persistent CTAs).
+// Units of work (I block x range of J blocks) are taken from a global
+// counter by persistent CTAs.
 #include <cuda_runtime.h>
 
 #include <climits>
 
 #include "ptx.cuh"
+#include "tail.cuh"
 #include "tiles.cuh"
 
 namespace cuapss {
@@ -38,13 +39,22 @@ constexpr int kKC = 32;                           // head features per slice
 constexpr int kSlice = kKC * kBlockRows;          // floats per slice (4096)
 constexpr int kSliceBytes = kSlice * 4;           // 16 KB
 constexpr int kAccLd = kBlockRows + 4;            // padded accumulator row
-constexpr size_t kSmemBytes = 4 * (size_t)kSliceBytes + (size_t)kBlockRows * kAccLd * 4 + 64;
+constexpr int kGCap = 5632;                       // I-block feature groups staged
+constexpr int kECap = 8704;                       // I-block tail postings staged
+constexpr size_t kSmemBytes = 4 * (size_t)kSliceBytes + (size_t)kBlockRows * kAccLd * 4 + 64 +
+                              (size_t)kGCap * 4 + ((size_t)kGCap + 1) * 4 + (size_t)kECap * 4 +
+                              (size_t)kECap + 16 + (size_t)kWarm * 2;
 
 struct Smem {
   float* a[2];
   float* b[2];
   float* acc;
   uint64_t* bar;
+  uint32_t* gf;
+  uint32_t* gs;
+  float* eu;
+  uint8_t* er;
+  uint16_t* warm;
 };
 
 __device__ __forceinline__ Smem carve(unsigned char* base) {
@@ -55,6 +65,11 @@ __device__ __forceinline__ Smem carve(unsigned char* base) {
   s.b[1] = s.b[0] + kSlice;
   s.acc = s.b[1] + kSlice;
   s.bar = reinterpret_cast<uint64_t*>(s.acc + kBlockRows * kAccLd);
+  s.gf = reinterpret_cast<uint32_t*>(s.bar + 8);
+  s.gs = s.gf + kGCap;
+  s.eu = reinterpret_cast<float*>(s.gs + kGCap + 1);
+  s.warm = reinterpret_cast<uint16_t*>(s.eu + kECap);
+  s.er = reinterpret_cast<uint8_t*>(s.warm + kWarm);
   return s;
 }
 
@@ -79,12 +94,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_tiles_fp32(const TileArgs A) {
     mbar_init(&S.bar[1], 1);
     fence_mbar_init();
   }
-  for (int i = tid; i < kBlockRows * kAccLd; i += kThreads) S.acc[i] = 0.0f;
+  for (int i = tid; i < kBlockRows * kAccLd; i += kThreads) reinterpret_cast<int*>(S.acc)[i] = 0;
   __syncthreads();
   uint32_t parity[2] = {0u, 0u};
   const int nchunks = A.p / kKC;
-  uint32_t* scr_cur = A.scr_cur + (int64_t)blockIdx.x * A.scr_stride;
-  uint32_t* scr_next = A.scr_next + (int64_t)blockIdx.x * A.scr_stride;
 
   for (;;) {
     if (tid == 0) s_unit = atomicAdd(A.unit_counter, 1);
@@ -92,63 +105,18 @@ __global__ void __launch_bounds__(kThreads, 1) k_tiles_fp32(const TileArgs A) {
     const int u = s_unit;
     __syncthreads();
     if (u >= A.nunits) break;
-    int blocks[2];
-    int nblk;
-    if (A.self) {
-      blocks[0] = u;
-      blocks[1] = A.nbI - 1 - u;
-      nblk = blocks[1] != blocks[0] ? 2 : 1;
-    } else {
-      blocks[0] = u;
-      nblk = 1;
-    }
-    for (int bi = 0; bi < nblk; ++bi) {
-      const int I = blocks[bi];
-      const int64_t row0 = (int64_t)I * kBlockRows;
-      const int rowsI = (int)(A.nI - row0 < kBlockRows ? A.nI - row0 : kBlockRows);
-      const int64_t e0 = A.tptrI[row0];
-      const int ne = (int)(A.tptrI[row0 + rowsI] - e0);
-      if (ne > A.scr_stride) {  // sized by the host from the largest block
-        if (tid == 0) atomicOr(A.err, kErrInternal);
-        return;
-      }
-      for (int e = tid; e < ne; e += kThreads) {
-        const uint32_t c = A.tcur0[e0 + e], end = A.tend[e0 + e];
-        scr_cur[e] = c;
-        scr_next[e] = c < end ? A.cscJ[c].x : 0xffffffffu;
-      }
-      __syncthreads();
-      const int Jbeg = A.self ? I : 0;
-      for (int J = Jbeg; J < A.nbJ; ++J) {
+    const int4 U = A.units[u];
+    const int I = U.x;
+    const int64_t row0 = (int64_t)I * kBlockRows;
+    const int rowsI = (int)(A.nI - row0 < kBlockRows ? A.nI - row0 : kBlockRows);
+    const TailI T = stage_tail_i<kThreads>(A, I, S.gf, S.gs, S.er, S.eu, S.warm, kGCap, kECap);
+    __syncthreads();
+    {
+      for (int J = U.y; J < U.z; ++J) {
         const int64_t col0 = (int64_t)J * kBlockRows;
-        const uint32_t j0 = (uint32_t)col0, j1 = (uint32_t)(col0 + kBlockRows);
         if (tid == 0 && nchunks > 0) issue_slice(S, 0, A.headI32, A.headJ32, I, J, A.p, 0);
-        // ---- tail: consume the postings of I's tail features that fall in J
-        for (int e = tid; e < ne; e += kThreads) {
-          uint32_t nr = scr_next[e];
-          if (nr < j1) {
-            const int r = A.tr[e0 + e];
-            const float uval = A.tu[e0 + e];
-            uint32_t cur = scr_cur[e];
-            const uint32_t end = A.tend[e0 + e];
-            uint2 pst = A.cscJ[cur];
-            for (;;) {
-              atomicAdd(&S.acc[r * kAccLd + (int)(pst.x - j0)], uval * __uint_as_float(pst.y));
-              ++cur;
-              if (cur >= end) {
-                nr = 0xffffffffu;
-                break;
-              }
-              pst = A.cscJ[cur];
-              if (pst.x >= j1) {
-                nr = pst.x;
-                break;
-              }
-            }
-            scr_cur[e] = cur;
-            scr_next[e] = nr;
-          }
-        }
+        // ---- tail: J's block-local postings probe I's feature groups
+        tail_tile(A, T, J, reinterpret_cast<int*>(S.acc), kAccLd, tid, kThreads);
         // ---- head: FP32 FMA chain over the p head features
         float h[8][8];
 #pragma unroll
@@ -190,11 +158,15 @@ __global__ void __launch_bounds__(kThreads, 1) k_tiles_fp32(const TileArgs A) {
 #pragma unroll
         for (int i = 0; i < 8; ++i) {
           const int r = (i < 4) ? ty * 4 + i : 64 + ty * 4 + (i - 4);
-          float4* arow = reinterpret_cast<float4*>(S.acc + r * kAccLd);
-          const float4 t0 = arow[tx], t1 = arow[16 + tx];
-          arow[tx] = make_float4(0.f, 0.f, 0.f, 0.f);
-          arow[16 + tx] = make_float4(0.f, 0.f, 0.f, 0.f);
-          const float tv[8] = {t0.x, t0.y, t0.z, t0.w, t1.x, t1.y, t1.z, t1.w};
+          int4* arow = reinterpret_cast<int4*>(S.acc + r * kAccLd);
+          const int4 t0 = arow[tx], t1 = arow[16 + tx];
+          arow[tx] = make_int4(0, 0, 0, 0);
+          arow[16 + tx] = make_int4(0, 0, 0, 0);
+          const float tv[8] = {
+              __int2float_rn(t0.x) * kTailUnscale, __int2float_rn(t0.y) * kTailUnscale,
+              __int2float_rn(t0.z) * kTailUnscale, __int2float_rn(t0.w) * kTailUnscale,
+              __int2float_rn(t1.x) * kTailUnscale, __int2float_rn(t1.y) * kTailUnscale,
+              __int2float_rn(t1.z) * kTailUnscale, __int2float_rn(t1.w) * kTailUnscale};
 #pragma unroll
           for (int j = 0; j < 8; ++j) {
             const int c = (j < 4) ? tx * 4 + j : 64 + tx * 4 + (j - 4);
@@ -233,9 +205,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_tiles_fp32(const TileArgs A) {
             }
           }
         }
-        __syncthreads();  // accumulator cleared, cursors advanced
+        __syncthreads();  // accumulator cleared
       }
     }
+    __syncthreads();  // staging buffers are rewritten by the next unit
   }
 }
 

@@ -8,42 +8,42 @@
 
 namespace cuapss {
 
-// Arguments shared by the pair-tile kernels. A "unit" is the work one CTA
-// takes from the global counter: for a self-join the row-block pair
-// (u, nb-1-u) (so every unit holds nb+1 tiles of the upper triangle), for a
-// cross-join one I block against every J block.
+// Arguments shared by the pair-tile kernels. A unit of work is one I row
+// block against a contiguous range [J0, J1) of J row blocks; the host cuts
+// heavy I blocks into short J ranges so that units cost about the same, and
+// the CTAs take units from a global counter.
 struct TileArgs {
   // I side (rows of the tile)
   const float* headI32;
   const void* headI16;
   int64_t nI;
   int nbI;
-  const int64_t* tptrI;
-  const uint32_t* tcur0;
-  const uint32_t* tend;
-  const uint8_t* tr;
-  const float* tu;
   const int32_t* blkmaxI;
   const float* hnormI;
+  const int64_t* gptrI;     // groups of each I block
+  const uint32_t* gstartI;  // entries of each group
+  const uint32_t* gfeatI;   // feature of each group
+  const uint32_t* bilI_f;
+  const uint8_t* bilI_r;
+  const float* bilI_u;
   // J side (columns of the tile)
   const float* headJ32;
   const void* headJ16;
   int64_t nJ;
   int nbJ;
-  const uint2* cscJ;
   const int32_t* blkmaxJ;
   const float* hnormJ;
+  const int64_t* bptrJ;     // block-local inverted list of each J block
+  const uint2* bilJ_rec;    // packed postings {feature << 8 | row, value bits}
   int p;
   int self;
   float t;
   double eps_c1;  // FP32 error margin of a tile: eps_c1 * min(maxnnz_I, maxnnz_J) + eps_c0
   double eps_c0;
   double eps_head;  // tensor-core path: extra margin per unit of ||a_h|| ||b_h||
+  const int4* units;  // {I, J0, J1, 0}
   int nunits;
   int* unit_counter;
-  uint32_t* scr_cur;
-  uint32_t* scr_next;
-  int64_t scr_stride;
   uint64_t* cand_key;
   float* cand_sim;
   unsigned long long* cand_count;
