@@ -122,10 +122,18 @@ cuapss_status join_device(cuapss_ctx* ctx, const DevCsr& a, const DevCsr* b, flo
   const int precision = ctx->opts.precision;
   int p = ctx->opts.head_width > 0 ? ctx->opts.head_width
                                    : choose_head_width(precision, a.n + bb.n, d, a.nnz + bb.nnz);
-  p = (int)std::min<int64_t>(((int64_t)p + 31) / 32 * 32, ((d + 31) / 32) * 32);
+  const bool mixed = precision == CUAPSS_PREC_MIXED;
+  const int pq = mixed ? 64 : 32;  // head width granularity of the tile kernels
+  p = (int)std::min<int64_t>(((int64_t)p + pq - 1) / pq * pq, ((d + pq - 1) / pq) * pq);
+  if (mixed && p < 64) p = 64;
   PrepOptions po;
   po.p = p;
-  po.want_head32 = 1;
+  // Rows keep the caller's order: a 128-row block of random rows carries a
+  // near-average tail, so the tail's shared-memory staging fits almost every
+  // block (grouping long rows together would overflow it).
+  po.row_sort = 0;
+  po.want_head32 = mixed ? 0 : 1;
+  po.want_head16 = mixed ? 1 : 0;
   Side SA, SB;
   SA.rp0 = a.rp;
   SA.col0 = a.col;
@@ -168,7 +176,7 @@ cuapss_status join_device(cuapss_ctx* ctx, const DevCsr& a, const DevCsr* b, flo
   ta.nbJ = SJ->nb;
   ta.blkmaxJ = SJ->blk_maxnnz;
   ta.hnormJ = SJ->hnorm;
-  ta.bptrJ = SJ->bptr;
+  ta.hptrJ = SJ->hptr;
   ta.bilJ_rec = SJ->bil_rec;
   ta.p = SA.p;
   ta.self = self ? 1 : 0;
@@ -179,6 +187,14 @@ cuapss_status join_device(cuapss_ctx* ctx, const DevCsr& a, const DevCsr* b, flo
   ta.eps_c1 = (u * nrm2 + std::ldexp(1.0, -31)) * 1.001;
   ta.eps_c0 = 3.0 * u * nrm2 * 1.001 + 1e-10;
   ta.eps_head = 0.0;
+  if (mixed) {
+    // BF16 inputs: each factor rounded to 8 significant bits (relative
+    // 2^-8), products exact in FP32; tensor-core accumulation over p/16
+    // steps bounded by 2^-20 relative per step.
+    ta.eps_head = (std::ldexp(1.0, -7) + std::ldexp(1.0, -16)) +
+                  (SA.p / 16.0 + 2.0) * std::ldexp(1.0, -20) * (1.0 + std::ldexp(1.0, -7));
+    ta.eps_head *= 1.001;
+  }
   // ---- units: I block x J range, heavy I blocks cut into short ranges ----
   const int grid_max = ctx->sms;
   std::vector<int4> units;
@@ -223,7 +239,10 @@ cuapss_status join_device(cuapss_ctx* ctx, const DevCsr& a, const DevCsr* b, flo
     CU_TRY(cudaMemsetAsync(unit_counter, 0, sizeof(int), st));
     CU_TRY(cudaMemsetAsync(err, 0, sizeof(int), st));
     CU_TRY(cudaMemsetAsync(ccount, 0, sizeof(unsigned long long), st));
-    if (ntiles > 0) ST_TRY(launch_tiles_fp32(ta, grid, st));
+    if (ntiles > 0) {
+      if (mixed) ST_TRY(launch_tiles_mma(ta, SA.head16, SJ->head16, SA.p, grid, st));
+      else ST_TRY(launch_tiles_fp32(ta, grid, st));
+    }
     unsigned long long hc = 0;
     int herr = 0;
     CU_TRY(cudaMemcpyAsync(&hc, ccount, sizeof(hc), cudaMemcpyDeviceToHost, st));

@@ -204,6 +204,28 @@ __global__ void k_head32_scatter(const int64_t* __restrict__ rp2, const int32_t*
   }
 }
 
+// BF16 head block, one 16 KB tile per (row block, 64-feature chunk): row rr
+// of the tile occupies bytes [128 rr, 128 rr + 128) and its 16-byte chunk c
+// (features 8c..8c+7 of the chunk) sits at chunk position c ^ (rr % 8), the
+// 128-byte swizzle the tensor core expects, so a plain bulk copy lands a tile
+// in shared memory ready for tcgen05.mma.
+__global__ void k_head16_scatter(const int64_t* __restrict__ rp2, const int32_t* __restrict__ col2,
+                                 const float* __restrict__ val2, const int32_t* __restrict__ hlen,
+                                 int64_t n, int nkc, __nv_bfloat16* __restrict__ head16) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t r = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; r < n; r += warps) {
+    const int64_t lo = rp2[r];
+    const int64_t b = r / kBlockRows, rr = r % kBlockRows;
+    for (int64_t e = lo + lane; e < lo + hlen[r]; e += 32) {
+      const int f = col2[e];
+      const int kc = f >> 6, c = (f >> 3) & 7, w = f & 7;
+      const int64_t off = (((b * nkc + kc) * kBlockRows + rr) * 128 + ((c ^ (int)(rr & 7)) * 16)) / 2 + w;
+      head16[off] = __float2bfloat16_rn(val2[e]);
+    }
+  }
+}
+
 // One warp per new row: tail entries in row order, sort keys for the
 // block-local lists (block, feature) and, optionally, the global lists
 // (feature, row); posting counts per tail feature.
@@ -213,13 +235,15 @@ __global__ void k_tail_entries(const int64_t* __restrict__ rp2, const int32_t* _
                                int fb, uint32_t* __restrict__ tk, uint8_t* __restrict__ tr,
                                float* __restrict__ tu, uint64_t* __restrict__ ckeys,
                                uint32_t* __restrict__ cvals, uint64_t* __restrict__ bkeys,
-                               uint32_t* __restrict__ bvals, int32_t* __restrict__ ccount) {
+                               uint32_t* __restrict__ bvals, uint64_t* __restrict__ hkeys,
+                               uint32_t* __restrict__ hvals, int32_t* __restrict__ ccount) {
   const int lane = threadIdx.x & 31;
   const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
   for (int64_t r = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; r < n; r += warps) {
     const int64_t lo = rp2[r] + hlen[r], hi = rp2[r + 1];
     const int64_t t0 = tptr[r];
     const uint64_t blk = (uint64_t)(r / kBlockRows);
+    const uint64_t hblk = (uint64_t)(r / (kBlockRows / 2));
     for (int64_t k = lo + lane; k < hi; k += 32) {
       const int64_t t = t0 + (k - lo);
       const int32_t f = col2[k] - p;
@@ -228,6 +252,8 @@ __global__ void k_tail_entries(const int64_t* __restrict__ rp2, const int32_t* _
       tu[t] = val2[k];
       bkeys[t] = (blk << fb) | (uint64_t)f;
       bvals[t] = (uint32_t)t;
+      hkeys[t] = (hblk << fb) | (uint64_t)f;
+      hvals[t] = (uint32_t)t;
       if (ckeys) {
         ckeys[t] = ((uint64_t)f << rbits) | (uint64_t)r;
         cvals[t] = (uint32_t)t;
@@ -240,8 +266,7 @@ __global__ void k_tail_entries(const int64_t* __restrict__ rp2, const int32_t* _
 __global__ void k_bil_fill(const uint64_t* __restrict__ keys, const uint32_t* __restrict__ vals,
                            const uint8_t* __restrict__ tr, const float* __restrict__ tu, int64_t T,
                            uint64_t fmask, uint32_t* __restrict__ bil_f, uint8_t* __restrict__ bil_r,
-                           float* __restrict__ bil_u, uint2* __restrict__ bil_rec,
-                           uint32_t* __restrict__ flags) {
+                           float* __restrict__ bil_u, uint32_t* __restrict__ flags) {
   for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < T;
        k += (int64_t)gridDim.x * blockDim.x) {
     const uint64_t key = keys[k];
@@ -250,9 +275,27 @@ __global__ void k_bil_fill(const uint64_t* __restrict__ keys, const uint32_t* __
     bil_f[k] = f;
     bil_r[k] = tr[t];
     bil_u[k] = tu[t];
-    bil_rec[k] = make_uint2((f << 8) | (uint32_t)tr[t], __float_as_uint(tu[t]));
     flags[k] = (k == 0 || keys[k - 1] != key) ? 1u : 0u;
   }
+}
+
+// Packed J-side postings in (half-block, feature, row) order.
+__global__ void k_rec_fill(const uint64_t* __restrict__ keys, const uint32_t* __restrict__ vals,
+                           const uint8_t* __restrict__ tr, const float* __restrict__ tu, int64_t T,
+                           uint64_t fmask, uint2* __restrict__ rec) {
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < T;
+       k += (int64_t)gridDim.x * blockDim.x) {
+    const uint32_t t = vals[k];
+    const uint32_t f = (uint32_t)(keys[k] & fmask);
+    rec[k] = make_uint2((f << 8) | (uint32_t)tr[t], __float_as_uint(tu[t]));
+  }
+}
+
+__global__ void k_half_ptrs(const int64_t* __restrict__ tptr, int64_t n, int nh,
+                            int64_t* __restrict__ hptr) {
+  for (int64_t h = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; h <= nh;
+       h += (int64_t)gridDim.x * blockDim.x)
+    hptr[h] = tptr[min(n, h * (kBlockRows / 2))];
 }
 
 __global__ void k_group_starts(const uint32_t* __restrict__ flags, const uint32_t* __restrict__ gidx,
@@ -375,8 +418,10 @@ cuapss_status build_side(Side& s, const PrepOptions& o, const int32_t* perm, Wor
                          const std::string& tag, cudaStream_t st) {
   const int64_t n = s.n, d = s.d, nnz = s.nnz;
   if (n >= INT32_MAX || nnz >= (int64_t)UINT32_MAX - 1) return CUAPSS_EINVAL;
-  s.p = (int)std::min<int64_t>(o.p, d);
-  if (o.want_head32) s.p = (int)std::min<int64_t>(o.p, ceil_div(d, 32) * 32);
+  // the dense head blocks are built in slices of 32 (FP32) or 64 (BF16)
+  // features; a head wider than d is padded with zero columns
+  const int64_t gran = o.want_head16 ? 64 : (o.want_head32 ? 32 : 1);
+  s.p = (int)std::min<int64_t>(o.p, ceil_div(d, gran) * gran);
   const int p = s.p;
   s.nb = (int)ceil_div(n, kBlockRows);
   const int nb = s.nb;
@@ -440,6 +485,17 @@ cuapss_status build_side(Side& s, const PrepOptions& o, const int32_t* perm, Wor
                                                                       s.hlen, n, p, s.head32);
     LAUNCH_CHECK();
   }
+  // ---- dense BF16 head block (tensor-core path) ----
+  if (o.want_head16 && p > 0) {
+    if (p % 64 != 0) return CUAPSS_EINVAL;
+    const int nkc = p / 64;
+    const size_t hb = (size_t)nb * nkc * kBlockRows * 64;
+    ST_TRY(ws.get(t + "head16", hb, &s.head16));
+    CU_TRY(cudaMemsetAsync(s.head16, 0, hb * sizeof(__nv_bfloat16), st));
+    k_head16_scatter<<<grid_for(n * 32, kThreads), kThreads, 0, st>>>(s.rp2, s.col2, s.val2,
+                                                                      s.hlen, n, nkc, s.head16);
+    LAUNCH_CHECK();
+  }
   // ---- tail: entries in row order, block-local inverted lists, groups ----
   CU_TRY(cudaMemcpyAsync(&s.ntail, s.tptr + n, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
   CU_TRY(cudaStreamSynchronize(st));
@@ -449,14 +505,16 @@ cuapss_status build_side(Side& s, const PrepOptions& o, const int32_t* perm, Wor
   if (nf >= (1 << 24)) return CUAPSS_EINVAL;  // packed postings hold 24-bit features
   const int fb = std::max(1, bits_for((uint64_t)nf));
   const int bb = std::max(1, bits_for((uint64_t)nb));
-  uint64_t *ckeys = nullptr, *bkeys = nullptr;
-  uint32_t *cvals = nullptr, *bvals = nullptr, *flags = nullptr;
+  uint64_t *ckeys = nullptr, *bkeys = nullptr, *hkeys = nullptr;
+  uint32_t *cvals = nullptr, *bvals = nullptr, *hvals = nullptr, *flags = nullptr;
   int32_t* ccount = nullptr;
   ST_TRY(ws.get(t + "tk", (size_t)T, &s.tk));
   ST_TRY(ws.get(t + "tr", (size_t)T, &s.tr));
   ST_TRY(ws.get(t + "tu", (size_t)T, &s.tu));
   ST_TRY(ws.get(t + "bkeys", (size_t)T, &bkeys));
   ST_TRY(ws.get(t + "bvals", (size_t)T, &bvals));
+  ST_TRY(ws.get(t + "hkeys", (size_t)T, &hkeys));
+  ST_TRY(ws.get(t + "hvals", (size_t)T, &hvals));
   ST_TRY(ws.get(t + "ccount", (size_t)nf + 1, &ccount));
   if (o.want_csc) {
     ST_TRY(ws.get(t + "ckeys", (size_t)T, &ckeys));
@@ -465,7 +523,7 @@ cuapss_status build_side(Side& s, const PrepOptions& o, const int32_t* perm, Wor
   CU_TRY(cudaMemsetAsync(ccount, 0, sizeof(int32_t) * (nf + 1), st));
   k_tail_entries<<<grid_for(n * 32, kThreads), kThreads, 0, st>>>(
       s.rp2, s.col2, s.val2, s.hlen, s.tptr, n, p, rbits, fb, s.tk, s.tr, s.tu, ckeys, cvals,
-      bkeys, bvals, ccount);
+      bkeys, bvals, hkeys, hvals, ccount);
   LAUNCH_CHECK();
   // block-local inverted lists: stable sort by (block, feature) keeps rows
   // ascending inside a feature; groups come from a scan of head flags
@@ -473,12 +531,24 @@ cuapss_status build_side(Side& s, const PrepOptions& o, const int32_t* perm, Wor
   ST_TRY(ws.get(t + "bil_f", (size_t)T, &s.bil_f));
   ST_TRY(ws.get(t + "bil_r", (size_t)T, &s.bil_r));
   ST_TRY(ws.get(t + "bil_u", (size_t)T, &s.bil_u));
-  ST_TRY(ws.get(t + "bil_rec", (size_t)T, &s.bil_rec));
   ST_TRY(ws.get(t + "gflags", (size_t)T + 1, &flags));
   k_bil_fill<<<grid_for(T, kThreads), kThreads, 0, st>>>(bkeys, bvals, s.tr, s.tu, T,
                                                         (1ull << fb) - 1, s.bil_f, s.bil_r,
-                                                        s.bil_u, s.bil_rec, flags);
+                                                        s.bil_u, flags);
   LAUNCH_CHECK();
+  // J-side postings: per 64-row half-block, sorted by feature, packed
+  {
+    const int nh = 2 * nb;  // half-blocks, the last one possibly empty
+    ST_TRY(radix_sort_pairs(hkeys, hvals, T, std::max(1, bits_for((uint64_t)nh)) + fb, ws,
+                            t + "rec", st));
+    ST_TRY(ws.get(t + "bil_rec", (size_t)T, &s.bil_rec));
+    ST_TRY(ws.get(t + "hptr", (size_t)nh + 1, &s.hptr));
+    k_rec_fill<<<grid_for(T, kThreads), kThreads, 0, st>>>(hkeys, hvals, s.tr, s.tu, T,
+                                                          (1ull << fb) - 1, s.bil_rec);
+    LAUNCH_CHECK();
+    k_half_ptrs<<<grid_for(nh + 1, kThreads), kThreads, 0, st>>>(s.tptr, n, nh, s.hptr);
+    LAUNCH_CHECK();
+  }
   uint32_t* gidx = nullptr;
   ST_TRY(ws.get(t + "gidx", (size_t)T + 1, &gidx));
   ST_TRY(exclusive_scan<uint32_t>(flags, gidx, T, gidx + T, ws, t + "gidx", st));

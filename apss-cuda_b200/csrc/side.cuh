@@ -22,6 +22,9 @@
 //   bil_f/bil_r/bil_u         block-local inverted lists: the tail postings
 //                             of each row block sorted by (feature, row):
 //                             feature - p, row inside the block, value
+//   bil_rec   uint2[T]        the same postings per 64-row half-block, sorted by
+//                             feature, packed {feature << 8 | row, value}
+//   hptr      int64[2nb+1]    postings of each half-block
 //   gstart    uint32[G+1]     feature groups: entries [gstart[g], gstart[g+1])
 //                             of the BIL share one feature
 //   gfeat     uint32[G]       feature of each group
@@ -65,7 +68,9 @@ struct Side {
   uint32_t* bil_f = nullptr;
   uint8_t* bil_r = nullptr;
   float* bil_u = nullptr;
-  uint2* bil_rec = nullptr;       // packed posting {feature << 8 | row, value bits}
+  uint2* bil_rec = nullptr;       // J-side postings per 64-row half-block, sorted by
+                                  // feature: {feature << 8 | row in block, value bits}
+  int64_t* hptr = nullptr;        // [2 nb + 1] postings of each half-block
   uint32_t* gstart = nullptr;
   uint32_t* gfeat = nullptr;      // feature of each group
   int64_t* gptr = nullptr;

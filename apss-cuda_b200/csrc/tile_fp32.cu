@@ -39,22 +39,23 @@ constexpr int kKC = 32;                           // head features per slice
 constexpr int kSlice = kKC * kBlockRows;          // floats per slice (4096)
 constexpr int kSliceBytes = kSlice * 4;           // 16 KB
 constexpr int kAccLd = kBlockRows + 4;            // padded accumulator row
-constexpr int kGCap = 5632;                       // I-block feature groups staged
-constexpr int kECap = 8704;                       // I-block tail postings staged
-constexpr size_t kSmemBytes = 4 * (size_t)kSliceBytes + (size_t)kBlockRows * kAccLd * 4 + 64 +
-                              (size_t)kGCap * 4 + ((size_t)kGCap + 1) * 4 + (size_t)kECap * 4 +
-                              (size_t)kECap + 16 + (size_t)kWarm * 2;
+constexpr int kECap = 7680;                       // I-block tail postings staged
+constexpr size_t kOffAcc = 4 * (size_t)kSliceBytes;
+constexpr size_t kOffBar = kOffAcc + (size_t)kBlockRows * kAccLd * 4;
+constexpr size_t kOffGf = kOffBar + 64;
+constexpr size_t kOffEu = kOffGf + (size_t)kECap * 4;
+constexpr size_t kOffBloom = kOffEu + (size_t)kECap * 4;
+constexpr size_t kOffWarm = kOffBloom + (size_t)kBloomWords * 4;
+constexpr size_t kOffGs = kOffWarm + (size_t)kWarm * 2;
+constexpr size_t kOffEr = kOffGs + ((size_t)kECap + 8) * 2;
+constexpr size_t kSmemBytes = kOffEr + (size_t)kECap;
 
 struct Smem {
   float* a[2];
   float* b[2];
   float* acc;
   uint64_t* bar;
-  uint32_t* gf;
-  uint32_t* gs;
-  float* eu;
-  uint8_t* er;
-  uint16_t* warm;
+  TailStage ts;
 };
 
 __device__ __forceinline__ Smem carve(unsigned char* base) {
@@ -63,13 +64,15 @@ __device__ __forceinline__ Smem carve(unsigned char* base) {
   s.a[1] = s.a[0] + kSlice;
   s.b[0] = s.a[1] + kSlice;
   s.b[1] = s.b[0] + kSlice;
-  s.acc = s.b[1] + kSlice;
-  s.bar = reinterpret_cast<uint64_t*>(s.acc + kBlockRows * kAccLd);
-  s.gf = reinterpret_cast<uint32_t*>(s.bar + 8);
-  s.gs = s.gf + kGCap;
-  s.eu = reinterpret_cast<float*>(s.gs + kGCap + 1);
-  s.warm = reinterpret_cast<uint16_t*>(s.eu + kECap);
-  s.er = reinterpret_cast<uint8_t*>(s.warm + kWarm);
+  s.acc = reinterpret_cast<float*>(base + kOffAcc);
+  s.bar = reinterpret_cast<uint64_t*>(base + kOffBar);
+  s.ts.gf = reinterpret_cast<uint32_t*>(base + kOffGf);
+  s.ts.eu = reinterpret_cast<float*>(base + kOffEu);
+  s.ts.bloom = reinterpret_cast<uint32_t*>(base + kOffBloom);
+  s.ts.warm = reinterpret_cast<uint16_t*>(base + kOffWarm);
+  s.ts.gs = reinterpret_cast<uint16_t*>(base + kOffGs);
+  s.ts.er = reinterpret_cast<uint8_t*>(base + kOffEr);
+  s.ts.ecap = kECap;
   return s;
 }
 
@@ -109,14 +112,27 @@ __global__ void __launch_bounds__(kThreads, 1) k_tiles_fp32(const TileArgs A) {
     const int I = U.x;
     const int64_t row0 = (int64_t)I * kBlockRows;
     const int rowsI = (int)(A.nI - row0 < kBlockRows ? A.nI - row0 : kBlockRows);
-    const TailI T = stage_tail_i<kThreads>(A, I, S.gf, S.gs, S.er, S.eu, S.warm, kGCap, kECap);
-    __syncthreads();
+    const int nch = tail_nchunks(A, I, kECap);
+    TailI T{};
+    if (nch == 1) T = stage_tail_chunk<kThreads, 0>(A, S.ts, I, 0, 1, tid);
     {
       for (int J = U.y; J < U.z; ++J) {
         const int64_t col0 = (int64_t)J * kBlockRows;
         if (tid == 0 && nchunks > 0) issue_slice(S, 0, A.headI32, A.headJ32, I, J, A.p, 0);
-        // ---- tail: J's block-local postings probe I's feature groups
-        tail_tile(A, T, J, reinterpret_cast<int*>(S.acc), kAccLd, tid, kThreads);
+        // ---- tail: J's postings probe I's staged feature groups
+        {
+          int* acc = reinterpret_cast<int*>(S.acc);
+          const int64_t k0 = A.hptrJ[2 * J], k1 = A.hptrJ[2 * J + 2];
+          if (nch == 1) {
+            tail_postings<16>(A, S.ts, T, k0, k1, acc, kAccLd, 0, tid, kThreads);
+          } else {
+            for (int c = 0; c < nch; ++c) {
+              const TailI Tc = stage_tail_chunk<kThreads, 0>(A, S.ts, I, c, nch, tid);
+              tail_postings<16>(A, S.ts, Tc, k0, k1, acc, kAccLd, 0, tid, kThreads);
+              __syncthreads();  // staging rewritten by the next chunk
+            }
+          }
+        }
         // ---- head: FP32 FMA chain over the p head features
         float h[8][8];
 #pragma unroll

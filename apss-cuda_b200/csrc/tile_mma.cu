@@ -1,0 +1,409 @@
+// Mixed-precision hybrid pair-tile kernel: BF16 head on the 5th-generation
+// tensor cores (tcgen05, FP32 accumulators in tensor memory), FP32 tail on
+// the CUDA cores, threshold epilogue with a proven error band.
+//
+// Head. The p most frequent features of every 128-row block are stored as a
+// dense BF16 block, pre-arranged in global memory in the 128-byte-swizzled
+// K-major layout the tensor core reads, so one 16 KB bulk (TMA) copy moves a
+// [128 rows x 64 features] operand tile straight into shared memory. For a
+// tile (I, J): D[128 x 128] = H_I * H_J^T, accumulated in tensor memory over
+// p/64 chunks (4 MMAs of K = 16 each). This replaces the reference's
+// per-pair sparse-dense head dot (similarity_apss_rest / similarity_join_rest,
+// fengyilin118/APSS-CUDA similarity_search.cu:441-506, 854-915).
+//
+// Warp roles (one CTA per SM, persistent over a static share of the units):
+//   warp 0       producer: bulk copies of I and J operand tiles into a
+//                kStages-deep shared-memory ring (mbarrier full/empty);
+//   warp 1       MMA: allocates 256 tensor-memory columns (two 128-column
+//                accumulators), one thread issues tcgen05.mma and commits;
+//   warps 2..9   tail + epilogue: the sparse tail of the tile in fixed point
+//                (tail.cuh), in two 64-column halves, then the accumulator is
+//                read with tcgen05.ld, head + tail is compared with
+//                t - eps(i, j) and candidates are compacted with a warp ballot.
+// eps(i, j) bounds BF16 input rounding (2^-8 relative per factor) and the
+// FP32 / fixed-point sums, so no pair with FP64 similarity >= t is dropped;
+// the finalize stage decides the band exactly in FP64.
+//
+// Every mbarrier wait is bounded; a timeout raises kErrTimeout, sets a
+// shared abort flag that the other roles poll, drains in-flight copies and
+// MMAs, frees tensor memory and returns.
+#include <cuda_runtime.h>
+
+#include "ptx.cuh"
+#include "tail.cuh"
+#include "tiles.cuh"
+
+namespace cuapss {
+
+namespace {
+
+constexpr int kCW = 16;                       // tail + epilogue warps (4 per lane quarter)
+constexpr int kCT = kCW * 32;                 // their threads
+constexpr int kThreads = 64 + kCT;            // + producer warp + MMA warp
+constexpr int kKC = 64;                       // BF16 features per chunk (128-byte rows)
+constexpr int kTileBytes = kBlockRows * kKC * 2;  // 16 KB per operand chunk
+constexpr int kStages = 3;
+constexpr int kAccCols = 64;                  // tail accumulator: half a tile
+constexpr int kAccLd = kAccCols + 1;          // odd stride: conflict-free row reads
+constexpr int kECap = 7680;                   // I-block tail postings staged per chunk
+constexpr uint32_t kTmemCols = 256;
+constexpr int kComputeBar = 1;
+constexpr int kBatch = 8;                     // J postings per thread per load batch
+constexpr int kEpiCols = kAccCols / (kCW / 4);  // tile columns per thread per half (16)
+
+struct SmemM {
+  uint8_t* stage;       // kStages x (A 16 KB | B 16 KB), 1024-byte aligned
+  int* acc;
+  float* hnj;
+  uint64_t* full;
+  uint64_t* empty;
+  uint64_t* tfull;
+  uint64_t* tempty;
+  uint64_t* drain;
+  uint32_t* tmem_base;
+  int* abort;
+  TailStage ts;
+};
+
+__host__ __device__ constexpr size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+struct Layout {
+  size_t acc, hnj, bars, tmem, abort, gf, eu, bloom, warm, gs, er, total;
+  __host__ __device__ constexpr Layout()
+      : acc(0), hnj(0), bars(0), tmem(0), abort(0), gf(0), eu(0), bloom(0), warm(0), gs(0), er(0),
+        total(0) {
+    size_t o = (size_t)kStages * 2 * kTileBytes;
+    acc = o;
+    o += (size_t)kBlockRows * kAccLd * 4;
+    hnj = align_up(o, 16);
+    o = hnj + (size_t)kBlockRows * 4;
+    bars = align_up(o, 16);
+    o = bars + (size_t)(2 * kStages + 5) * 8;
+    tmem = align_up(o, 16);
+    o = tmem + 16;
+    abort = o;
+    o += 16;
+    gf = align_up(o, 16);
+    o = gf + (size_t)kECap * 4;
+    eu = align_up(o, 16);
+    o = eu + (size_t)kECap * 4;
+    bloom = align_up(o, 16);
+    o = bloom + (size_t)kBloomWords * 4;
+    warm = align_up(o, 16);
+    o = warm + (size_t)kWarm * 2;
+    gs = align_up(o, 16);
+    o = gs + ((size_t)kECap + 8) * 2;
+    er = align_up(o, 16);
+    o = er + (size_t)kECap;
+    total = align_up(o, 16);
+  }
+};
+constexpr Layout kLayout{};
+constexpr size_t kSmemBytes = kLayout.total + 1024;  // + alignment slack
+static_assert(kSmemBytes <= 232448, "shared memory budget");
+
+__device__ __forceinline__ SmemM carve(uint8_t* raw) {
+  uint8_t* base = reinterpret_cast<uint8_t*>(align_up(reinterpret_cast<size_t>(raw), 1024));
+  SmemM s;
+  s.stage = base;
+  s.acc = reinterpret_cast<int*>(base + kLayout.acc);
+  s.hnj = reinterpret_cast<float*>(base + kLayout.hnj);
+  uint64_t* b = reinterpret_cast<uint64_t*>(base + kLayout.bars);
+  s.full = b;
+  s.empty = b + kStages;
+  s.tfull = b + 2 * kStages;
+  s.tempty = b + 2 * kStages + 2;
+  s.drain = b + 2 * kStages + 4;
+  s.tmem_base = reinterpret_cast<uint32_t*>(base + kLayout.tmem);
+  s.abort = reinterpret_cast<int*>(base + kLayout.abort);
+  s.ts.gf = reinterpret_cast<uint32_t*>(base + kLayout.gf);
+  s.ts.eu = reinterpret_cast<float*>(base + kLayout.eu);
+  s.ts.bloom = reinterpret_cast<uint32_t*>(base + kLayout.bloom);
+  s.ts.warm = reinterpret_cast<uint16_t*>(base + kLayout.warm);
+  s.ts.gs = reinterpret_cast<uint16_t*>(base + kLayout.gs);
+  s.ts.er = base + kLayout.er;
+  s.ts.ecap = kECap;
+  return s;
+}
+
+// Bounded wait that also gives up when another role raised the abort flag.
+__device__ __forceinline__ bool wait_or_abort(uint64_t* bar, uint32_t parity,
+                                              const volatile int* abort) {
+  for (uint32_t i = 0; i < kMaxPolls; ++i) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if ((i & 31u) == 31u && *abort) return false;
+  }
+  return false;
+}
+
+__device__ __forceinline__ void raise_abort(const TileArgs& A, volatile int* abort) {
+  if (!*abort) {
+    *abort = 1;
+    atomicOr(A.err, kErrTimeout);
+  }
+}
+
+struct MmaArgs {
+  const uint8_t* headI16;
+  const uint8_t* headJ16;
+  int nkc;  // p / 64
+};
+
+__global__ void __launch_bounds__(kThreads, 1) k_tiles_mma(const TileArgs A, const MmaArgs M) {
+  extern __shared__ uint8_t smem_raw[];
+  const SmemM S = carve(smem_raw);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  volatile int* abort = S.abort;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kStages; ++s) {
+      mbar_init(&S.full[s], 1);
+      mbar_init(&S.empty[s], 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&S.tfull[b], 1);
+      mbar_init(&S.tempty[b], kCW);
+    }
+    mbar_init(S.drain, 1);
+    *abort = 0;
+    fence_mbar_init();
+  }
+  if (warp == 1) {
+    tmem_alloc(S.tmem_base, kTmemCols);
+    tmem_relinquish();
+  }
+  if (warp >= 2)
+    for (int i = threadIdx.x - 64; i < kBlockRows * kAccLd; i += kCT) S.acc[i] = 0;
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *S.tmem_base;
+
+  if (warp == 0) {
+    // ------------------------------------------------------------ producer
+    if (lane == 0) {
+      uint32_t it = 0;
+      bool ok = true;
+      for (int u = blockIdx.x; ok && u < A.nunits; u += gridDim.x) {
+        const int4 U = A.units[u];
+        for (int J = U.y; ok && J < U.z; ++J) {
+          for (int kc = 0; kc < M.nkc; ++kc, ++it) {
+            const uint32_t s = it % kStages, round = it / kStages;
+            if (!wait_or_abort(&S.empty[s], (round & 1u) ^ 1u, abort)) {
+              raise_abort(A, abort);
+              ok = false;
+              break;
+            }
+            uint8_t* dst = S.stage + (size_t)s * 2 * kTileBytes;
+            mbar_arrive_expect_tx(&S.full[s], 2 * kTileBytes);
+            bulk_g2s(dst, M.headI16 + ((size_t)U.x * M.nkc + kc) * kTileBytes, kTileBytes,
+                     &S.full[s]);
+            bulk_g2s(dst + kTileBytes, M.headJ16 + ((size_t)J * M.nkc + kc) * kTileBytes,
+                     kTileBytes, &S.full[s]);
+          }
+        }
+      }
+      // drain: the last copies issued must have landed before the CTA exits
+      const uint32_t first = it > (uint32_t)kStages ? it - kStages : 0u;
+      for (uint32_t q = first; q < it; ++q)
+        mbar_wait(&S.full[q % kStages], (q / kStages) & 1u);
+    }
+    __syncwarp();
+  } else if (warp == 1) {
+    // ----------------------------------------------------------------- MMA
+    if (lane == 0) {
+      const uint32_t idesc = umma_idesc_bf16(kBlockRows, kBlockRows);
+      uint32_t it = 0, tt = 0;
+      bool ok = true;
+      for (int u = blockIdx.x; ok && u < A.nunits; u += gridDim.x) {
+        const int4 U = A.units[u];
+        for (int J = U.y; ok && J < U.z; ++J, ++tt) {
+          const uint32_t b = tt & 1u, tround = tt >> 1;
+          if (!wait_or_abort(&S.tempty[b], (tround & 1u) ^ 1u, abort)) {
+            raise_abort(A, abort);
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t d = tmem + b * (uint32_t)kBlockRows;
+          for (int kc = 0; kc < M.nkc; ++kc, ++it) {
+            const uint32_t s = it % kStages, round = it / kStages;
+            if (!wait_or_abort(&S.full[s], round & 1u, abort)) {
+              raise_abort(A, abort);
+              ok = false;
+              break;
+            }
+            tc_fence_after();
+            const uint8_t* st = S.stage + (size_t)s * 2 * kTileBytes;
+            const uint64_t ad = umma_desc_sw128(st);
+            const uint64_t bd = umma_desc_sw128(st + kTileBytes);
+#pragma unroll
+            for (int k = 0; k < kKC / 16; ++k)
+              umma_bf16(d, ad + 2u * k, bd + 2u * k, idesc, (kc | k) != 0 ? 1u : 0u);
+            umma_commit(&S.empty[s]);
+          }
+          if (ok) umma_commit(&S.tfull[b]);
+        }
+      }
+      // drain: every MMA issued must be complete before tensor memory is freed
+      if (it > 0) {
+        umma_commit(S.drain);
+        mbar_wait(S.drain, 0);
+      }
+    }
+    __syncwarp();
+  } else {
+    // ---------------------------------------------- tail + epilogue warps
+    // The J postings of the next half-tile are loaded into registers before
+    // the current epilogue, so their latency hides behind it.
+    const int ctid = threadIdx.x - 64;
+    const int q = warp & 3;             // tensor-memory lane quarter of this warp
+    const int colq = (warp - 2) >> 2;   // which kEpiCols of each 64 columns
+    const int row = 32 * q + lane;
+    uint32_t tt = 0;
+    bool ok = true;
+    TailBatch<kBatch> B;
+    if ((int)blockIdx.x < A.nunits) {
+      const int J0 = A.units[blockIdx.x].y;
+      tail_prefetch(A, B, A.hptrJ[2 * J0], A.hptrJ[2 * J0 + 1], ctid, kCT);
+    }
+    for (int u = blockIdx.x; ok && u < A.nunits; u += gridDim.x) {
+      const int4 U = A.units[u];
+      const int I = U.x;
+      const int64_t row0 = (int64_t)I * kBlockRows;
+      const int rowsI = (int)(A.nI - row0 < kBlockRows ? A.nI - row0 : kBlockRows);
+      named_bar(kComputeBar, kCT);
+      const int nch = tail_nchunks(A, I, kECap);
+      TailI T{};
+      if (nch == 1) T = stage_tail_chunk<kCT, kComputeBar>(A, S.ts, I, 0, 1, ctid);
+      const float hn_r = row < rowsI ? A.hnormI[row0 + row] : 0.0f;
+      for (int J = U.y; ok && J < U.z; ++J, ++tt) {
+        const uint32_t b = tt & 1u, tround = tt >> 1;
+        const int64_t col0 = (int64_t)J * kBlockRows;
+        const int colsJ = (int)(A.nJ - col0 < kBlockRows ? A.nJ - col0 : kBlockRows);
+        const bool diag = A.self && (I == J);
+        const int kmax = min(A.blkmaxI[I], A.blkmaxJ[J]);
+        const float t_lo = __double2float_rd((double)A.t - (A.eps_c1 * kmax + A.eps_c0));
+        if (ctid < kBlockRows)
+          S.hnj[ctid] =
+              ctid < colsJ ? __double2float_ru(A.eps_head * (double)A.hnormJ[col0 + ctid]) : 0.0f;
+        for (int h = 0; h < 2; ++h) {
+          // ---- tail of this half-tile (its first batch is already in B)
+          if (nch == 1) {
+            tail_postings_pre<kBatch>(A, S.ts, T, B, S.acc, kAccLd, h * kAccCols, ctid, kCT);
+          } else {
+            for (int c = 0; c < nch; ++c) {
+              const TailI Tc = stage_tail_chunk<kCT, kComputeBar>(A, S.ts, I, c, nch, ctid);
+              tail_postings_pre<kBatch>(A, S.ts, Tc, B, S.acc, kAccLd, h * kAccCols, ctid, kCT);
+              named_bar(kComputeBar, kCT);  // staging rewritten by the next chunk
+            }
+          }
+          named_bar(kComputeBar, kCT);
+          if (h == 0) {
+            const bool got = wait_or_abort(&S.tfull[b], tround & 1u, abort);
+            if (named_bar_or(kComputeBar, kCT, !got)) {
+              raise_abort(A, abort);
+              ok = false;
+              break;
+            }
+            tc_fence_after();
+          }
+          // ---- prefetch the next half-tile's postings
+          {
+            int nJ = -1, nh = 0;
+            if (h == 0) {
+              nJ = J;
+              nh = 1;
+            } else if (J + 1 < U.z) {
+              nJ = J + 1;
+            } else if (u + (int)gridDim.x < A.nunits) {
+              nJ = A.units[u + gridDim.x].y;
+            }
+            if (nJ >= 0)
+              tail_prefetch(A, B, A.hptrJ[2 * nJ + nh], A.hptrJ[2 * nJ + nh + 1], ctid, kCT);
+          }
+          // ---- epilogue: head (tensor memory) + tail (shared) vs t - eps
+          const int cbase = h * kAccCols + colq * kEpiCols;  // first tile column of this thread
+          uint32_t v[kEpiCols];
+          tmem_ld16(tmem + b * (uint32_t)kBlockRows + (uint32_t)cbase + ((uint32_t)(32 * q) << 16),
+                    v);
+          uint32_t pass = 0;
+          int* arow = S.acc + row * kAccLd + colq * kEpiCols;
+          const bool row_ok = row < rowsI;
+          const bool simple = !diag && colsJ == kBlockRows;
+#pragma unroll
+          for (int j = 0; j < kEpiCols; ++j) {
+            const int c = cbase + j;
+            const int tq = arow[j];
+            arow[j] = 0;
+            const float s = fmaf(__int2float_rn(tq), kTailUnscale, __uint_as_float(v[j]));
+            v[j] = __float_as_uint(s);
+            const float thr = __fmaf_rd(-hn_r, S.hnj[c], t_lo);
+            bool okp = (s >= thr) && row_ok;
+            if (!simple) okp = okp && (c < colsJ) && (!diag || c > row);
+            pass |= (uint32_t)okp << j;
+          }
+          if (__any_sync(0xffffffffu, pass != 0u)) {
+            const int mine = __popc(pass);
+            int incl = mine;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+              const int x = __shfl_up_sync(0xffffffffu, incl, o);
+              if (lane >= o) incl += x;
+            }
+            const int total = __shfl_sync(0xffffffffu, incl, 31);
+            unsigned long long base = 0;
+            if (lane == 31) base = atomicAdd(A.cand_count, (unsigned long long)total);
+            base = __shfl_sync(0xffffffffu, base, 31);
+            unsigned long long w = base + (unsigned long long)(incl - mine);
+#pragma unroll
+            for (int j = 0; j < kEpiCols; ++j) {
+              if ((pass >> j) & 1u) {
+                if ((int64_t)w < A.cand_cap) {
+                  A.cand_key[w] =
+                      ((uint64_t)(row0 + row) << 32) | (uint64_t)(col0 + cbase + j);
+                  A.cand_sim[w] = __uint_as_float(v[j]);
+                }
+                ++w;
+              }
+            }
+          }
+          named_bar(kComputeBar, kCT);  // accumulator half cleared
+        }
+        if (!ok) break;
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&S.tempty[b]);
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    tc_fence_after();
+    tmem_dealloc(tmem, kTmemCols);
+  }
+}
+
+}  // namespace
+
+cuapss_status launch_tiles_mma(const TileArgs& a, const void* headI16, const void* headJ16,
+                               int p, int grid, cudaStream_t st) {
+  static bool attr_set = false;
+  if (!attr_set) {
+    CU_TRY(cudaFuncSetAttribute(k_tiles_mma, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)kSmemBytes));
+    attr_set = true;
+  }
+  if (p <= 0 || p % kKC != 0) return CUAPSS_EINVAL;
+  MmaArgs m;
+  m.headI16 = static_cast<const uint8_t*>(headI16);
+  m.headJ16 = static_cast<const uint8_t*>(headJ16);
+  m.nkc = p / kKC;
+  k_tiles_mma<<<grid, kThreads, kSmemBytes, st>>>(a, m);
+  LAUNCH_CHECK();
+  return CUAPSS_OK;
+}
+
+size_t tiles_mma_smem_bytes() { return kSmemBytes; }
+
+}  // namespace cuapss

@@ -33,7 +33,7 @@ struct TileArgs {
   int nbJ;
   const int32_t* blkmaxJ;
   const float* hnormJ;
-  const int64_t* bptrJ;     // block-local inverted list of each J block
+  const int64_t* hptrJ;     // postings of each 64-row half-block of J
   const uint2* bilJ_rec;    // packed postings {feature << 8 | row, value bits}
   int p;
   int self;
@@ -55,6 +55,13 @@ struct TileArgs {
 // row tiles; tail: inverted-list scan into shared-memory accumulators).
 cuapss_status launch_tiles_fp32(const TileArgs& a, int grid, cudaStream_t st);
 int tiles_fp32_max_grid();
+
+// Mixed-precision tile kernel (BF16 head on tcgen05 tensor cores, FP32 tail).
+// headI16 / headJ16: BF16 head blocks in the swizzled layout of
+// build_side; p a multiple of 64.
+cuapss_status launch_tiles_mma(const TileArgs& a, const void* headI16, const void* headJ16,
+                               int p, int grid, cudaStream_t st);
+size_t tiles_mma_smem_bytes();
 
 struct FinalizeArgs {
   const uint64_t* cand_key;
