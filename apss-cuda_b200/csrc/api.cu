@@ -170,6 +170,8 @@ cuapss_status join_device(cuapss_ctx* ctx, const DevCsr& a, const DevCsr* b, flo
   ta.gptrI = SA.gptr;
   ta.gstartI = SA.gstart;
   ta.gfeatI = SA.gfeat;
+  ta.chunk_ptrI = SA.chunk_ptr;
+  ta.chunk_gI = SA.chunk_g;
   ta.bilI_f = SA.bil_f;
   ta.bilI_r = SA.bil_r;
   ta.bilI_u = SA.bil_u;
@@ -186,6 +188,7 @@ cuapss_status join_device(cuapss_ctx* ctx, const DevCsr& a, const DevCsr* b, flo
   // FP32 head chain + fixed-point tail (2^-30 grid, exact sums) + final add:
   // |s~ - s| <= (K + 3) u ||a|| ||b|| + K 2^-31, K = shared features
   if (nrm2 >= 1.9) return CUAPSS_EINVAL;  // fixed-point tail needs ~unit norms
+  if (d - SA.p > (int64_t)(1u << 20) - 2) return CUAPSS_EINVAL;  // 20-bit tail feature keys
   ta.eps_c1 = (u * nrm2 + std::ldexp(1.0, -31)) * 1.001;
   ta.eps_c0 = 3.0 * u * nrm2 * 1.001 + 1e-10;
   ta.eps_head = 0.0;
@@ -197,7 +200,9 @@ cuapss_status join_device(cuapss_ctx* ctx, const DevCsr& a, const DevCsr* b, flo
                   (SA.p / 16.0 + 2.0) * std::ldexp(1.0, -20) * (1.0 + std::ldexp(1.0, -7));
     ta.eps_head *= 1.001;
   }
-  // ---- units: I block x J range, heavy I blocks cut into short ranges ----
+  // ---- units: I block x J range; an I block's J range is cut into chunks
+  // of about equal cost (about 16 units per CTA), heavier blocks get shorter
+  // ranges. CTAs take units round-robin (mixed kernel) or from a counter.
   const int grid_max = ctx->sms;
   std::vector<int4> units;
   {
@@ -211,9 +216,11 @@ cuapss_status join_device(cuapss_ctx* ctx, const DevCsr& a, const DevCsr* b, flo
     for (int I = 0; I < SA.nb; ++I) {
       const int jb = self ? I : 0, je = SJ->nb;
       const int chunk = (int)std::max(1.0, std::floor(target / weight(I)));
-      for (int j0 = jb; j0 < je; j0 += chunk) units.push_back(make_int4(I, j0, std::min(je, j0 + chunk), 0));
+      for (int j0 = jb; j0 < je; j0 += chunk)
+        units.push_back(make_int4(I, j0, std::min(je, j0 + chunk), 0));
     }
   }
+  const int grid = std::max(1, std::min((int)units.size(), grid_max));
   int4* d_units = nullptr;
   ST_TRY(ws.get("tiles:units", std::max<size_t>(units.size(), 1), &d_units));
   if (!units.empty())
@@ -228,7 +235,6 @@ cuapss_status join_device(cuapss_ctx* ctx, const DevCsr& a, const DevCsr* b, flo
   ST_TRY(ws.get("tiles:unit", 1, &unit_counter));
   ST_TRY(ws.get("tiles:err", 1, &err));
   ST_TRY(ws.get("tiles:ccount", 1, &ccount));
-  const int grid = std::max(1, std::min(ta.nunits, grid_max));
   ta.unit_counter = unit_counter;
   ta.err = err;
   ta.cand_count = ccount;

@@ -53,6 +53,10 @@ enum : int {
 };
 
 constexpr int kBlockRows = 128;  // rows per row block (tile edge)
+// Tail staging capacity of the tile kernels: a block's feature groups are
+// staged in shared memory in chunks of at most this many groups / postings.
+constexpr int kChunkGroups = 4096;
+constexpr int kChunkPostings = 8192;
 
 inline int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
 

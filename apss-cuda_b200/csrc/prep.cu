@@ -298,6 +298,34 @@ __global__ void k_half_ptrs(const int64_t* __restrict__ tptr, int64_t n, int nh,
     hptr[h] = tptr[min(n, h * (kBlockRows / 2))];
 }
 
+// Staging chunks of each block's feature groups: a chunk holds at most
+// kChunkGroups groups and kChunkPostings postings (one thread per block).
+template <bool FILL>
+__global__ void k_chunk_bounds(const int64_t* __restrict__ gptr, const uint32_t* __restrict__ gstart,
+                               int nb, int64_t* __restrict__ count,
+                               const int64_t* __restrict__ cptr, int64_t* __restrict__ bnd) {
+  for (int64_t b = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; b < nb;
+       b += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t g0 = gptr[b], g1 = gptr[b + 1];
+    int64_t s = g0, k = 0;
+    if (FILL) bnd[cptr[b]] = g0;
+    while (s < g1) {
+      const int64_t e1 = min(g1, s + (int64_t)kChunkGroups);
+      const uint32_t lim = gstart[s] + (uint32_t)kChunkPostings;
+      int64_t lo = s + 1, hi = e1;  // largest e in [s+1, e1] with gstart[e] <= lim
+      while (lo < hi) {
+        const int64_t mid = (lo + hi + 1) >> 1;
+        if (gstart[mid] <= lim) lo = mid;
+        else hi = mid - 1;
+      }
+      s = lo;
+      ++k;
+      if (FILL) bnd[cptr[b] + k] = s;
+    }
+    if (!FILL) count[b] = k + 1;  // chunk boundaries of block b (an empty block: 1)
+  }
+}
+
 __global__ void k_group_starts(const uint32_t* __restrict__ flags, const uint32_t* __restrict__ gidx,
                                const uint32_t* __restrict__ bil_f, int64_t T,
                                uint32_t* __restrict__ gstart, uint32_t* __restrict__ gfeat) {
@@ -566,6 +594,24 @@ cuapss_status build_side(Side& s, const PrepOptions& o, const int32_t* perm, Wor
   k_block_ptrs<<<grid_for(nb + 1, kThreads), kThreads, 0, st>>>(s.tptr, gidx, n, nb, s.bptr,
                                                                  s.gptr);
   LAUNCH_CHECK();
+  // ---- staging chunks of every block ----
+  {
+    int64_t* ccnt = nullptr;
+    ST_TRY(ws.get(t + "chunk_cnt", (size_t)nb + 1, &ccnt));
+    ST_TRY(ws.get(t + "chunk_ptr", (size_t)nb + 1, &s.chunk_ptr));
+    k_chunk_bounds<false><<<grid_for(nb, 128), 128, 0, st>>>(s.gptr, s.gstart, nb, ccnt, nullptr,
+                                                             nullptr);
+    LAUNCH_CHECK();
+    ST_TRY(exclusive_scan<int64_t>(ccnt, s.chunk_ptr, nb, s.chunk_ptr + nb, ws, t + "chunk", st));
+    int64_t total = 0;
+    CU_TRY(cudaMemcpyAsync(&total, s.chunk_ptr + nb, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+    CU_TRY(cudaStreamSynchronize(st));
+    ST_TRY(ws.get(t + "chunk_g", (size_t)std::max<int64_t>(total, 1), &s.chunk_g));
+    k_chunk_bounds<true><<<grid_for(nb, 128), 128, 0, st>>>(s.gptr, s.gstart, nb, nullptr,
+                                                            s.chunk_ptr, s.chunk_g);
+    LAUNCH_CHECK();
+    s.nchunk_bounds = total;
+  }
   // ---- global inverted lists (feature, row), on request ----
   if (o.want_csc) {
     uint32_t* entpos = nullptr;

@@ -5,9 +5,11 @@
 
 namespace cuapss {
 
-// Upper bound on polls of one mbarrier phase before a kernel gives up and
-// reports kErrTimeout (each poll may suspend the thread briefly).
-constexpr uint32_t kMaxPolls = 1u << 25;
+// A waiting thread sleeps in mbarrier.try_wait for up to kSuspendNs per poll
+// (it is woken as soon as the phase completes); after kMaxPolls polls (about
+// 2 s) the wait gives up and the kernel reports kErrTimeout.
+constexpr uint32_t kSuspendNs = 20000;
+constexpr uint32_t kMaxPolls = 100000;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return (uint32_t)__cvta_generic_to_shared(p);
@@ -40,10 +42,10 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
   uint32_t ok;
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
-      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
       "selp.u32 %0, 1, 0, p;\n\t}"
       : "=r"(ok)
-      : "r"(smem_u32(bar)), "r"(parity)
+      : "r"(smem_u32(bar)), "r"(parity), "r"(kSuspendNs)
       : "memory");
   return ok != 0;
 }

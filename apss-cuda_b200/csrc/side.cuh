@@ -29,6 +29,8 @@
 //                             of the BIL share one feature
 //   gfeat     uint32[G]       feature of each group
 //   gptr      int64[nb+1]     groups of each row block
+//   chunk_ptr/chunk_g         staging chunks of each block (at most
+//                             kChunkGroups groups, kChunkPostings postings)
 #pragma once
 
 #include <cuda_bf16.h>
@@ -73,6 +75,9 @@ struct Side {
   int64_t* hptr = nullptr;        // [2 nb + 1] postings of each half-block
   uint32_t* gstart = nullptr;
   uint32_t* gfeat = nullptr;      // feature of each group
+  int64_t* chunk_ptr = nullptr;   // [nb+1] staging-chunk boundaries of each block
+  int64_t* chunk_g = nullptr;     // boundaries (group indices), nchunks+1 per block
+  int64_t nchunk_bounds = 0;
   int64_t* gptr = nullptr;
   int64_t ngroups = 0;
   int64_t max_block_groups = 0;

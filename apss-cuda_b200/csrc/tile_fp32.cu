@@ -39,16 +39,14 @@ constexpr int kKC = 32;                           // head features per slice
 constexpr int kSlice = kKC * kBlockRows;          // floats per slice (4096)
 constexpr int kSliceBytes = kSlice * 4;           // 16 KB
 constexpr int kAccLd = kBlockRows + 4;            // padded accumulator row
-constexpr int kECap = 7680;                       // I-block tail postings staged
 constexpr size_t kOffAcc = 4 * (size_t)kSliceBytes;
 constexpr size_t kOffBar = kOffAcc + (size_t)kBlockRows * kAccLd * 4;
-constexpr size_t kOffGf = kOffBar + 64;
-constexpr size_t kOffEu = kOffGf + (size_t)kECap * 4;
-constexpr size_t kOffBloom = kOffEu + (size_t)kECap * 4;
-constexpr size_t kOffWarm = kOffBloom + (size_t)kBloomWords * 4;
-constexpr size_t kOffGs = kOffWarm + (size_t)kWarm * 2;
-constexpr size_t kOffEr = kOffGs + ((size_t)kECap + 8) * 2;
-constexpr size_t kSmemBytes = kOffEr + (size_t)kECap;
+constexpr size_t kOffHash = kOffBar + 64;                       // 16-byte aligned
+constexpr size_t kOffEu = kOffHash + (size_t)kBuckets * 16;
+constexpr size_t kOffGs = kOffEu + (size_t)kChunkPostings * 4;
+constexpr size_t kOffEr = kOffGs + ((size_t)kChunkGroups + 8) * 2;
+constexpr size_t kSmemBytes = kOffEr + (size_t)kChunkPostings;
+static_assert(kSmemBytes + 256 <= 232448, "shared memory budget");
 
 struct Smem {
   float* a[2];
@@ -66,13 +64,11 @@ __device__ __forceinline__ Smem carve(unsigned char* base) {
   s.b[1] = s.b[0] + kSlice;
   s.acc = reinterpret_cast<float*>(base + kOffAcc);
   s.bar = reinterpret_cast<uint64_t*>(base + kOffBar);
-  s.ts.gf = reinterpret_cast<uint32_t*>(base + kOffGf);
+  s.ts.hash = reinterpret_cast<uint4*>(base + kOffHash);
   s.ts.eu = reinterpret_cast<float*>(base + kOffEu);
-  s.ts.bloom = reinterpret_cast<uint32_t*>(base + kOffBloom);
-  s.ts.warm = reinterpret_cast<uint16_t*>(base + kOffWarm);
   s.ts.gs = reinterpret_cast<uint16_t*>(base + kOffGs);
   s.ts.er = reinterpret_cast<uint8_t*>(base + kOffEr);
-  s.ts.ecap = kECap;
+  s.ts.ecap = kChunkPostings;
   return s;
 }
 
@@ -109,12 +105,13 @@ __global__ void __launch_bounds__(kThreads, 1) k_tiles_fp32(const TileArgs A) {
     __syncthreads();
     if (u >= A.nunits) break;
     const int4 U = A.units[u];
+    if (U.y >= U.z) continue;
     const int I = U.x;
     const int64_t row0 = (int64_t)I * kBlockRows;
     const int rowsI = (int)(A.nI - row0 < kBlockRows ? A.nI - row0 : kBlockRows);
-    const int nch = tail_nchunks(A, I, kECap);
+    const int nch = tail_nchunks(A, I);
     TailI T{};
-    if (nch == 1) T = stage_tail_chunk<kThreads, 0>(A, S.ts, I, 0, 1, tid);
+    if (nch == 1) T = stage_tail_chunk<kThreads, 0>(A, S.ts, I, 0, tid);
     {
       for (int J = U.y; J < U.z; ++J) {
         const int64_t col0 = (int64_t)J * kBlockRows;
@@ -124,11 +121,11 @@ __global__ void __launch_bounds__(kThreads, 1) k_tiles_fp32(const TileArgs A) {
           int* acc = reinterpret_cast<int*>(S.acc);
           const int64_t k0 = A.hptrJ[2 * J], k1 = A.hptrJ[2 * J + 2];
           if (nch == 1) {
-            tail_postings<16>(A, S.ts, T, k0, k1, acc, kAccLd, 0, tid, kThreads);
+            tail_postings<8>(A, S.ts, T, k0, k1, acc, kAccLd, 0, tid, kThreads);
           } else {
             for (int c = 0; c < nch; ++c) {
-              const TailI Tc = stage_tail_chunk<kThreads, 0>(A, S.ts, I, c, nch, tid);
-              tail_postings<16>(A, S.ts, Tc, k0, k1, acc, kAccLd, 0, tid, kThreads);
+              const TailI Tc = stage_tail_chunk<kThreads, 0>(A, S.ts, I, c, tid);
+              tail_postings<8>(A, S.ts, Tc, k0, k1, acc, kAccLd, 0, tid, kThreads);
               __syncthreads();  // staging rewritten by the next chunk
             }
           }

@@ -45,10 +45,9 @@ constexpr int kTileBytes = kBlockRows * kKC * 2;  // 16 KB per operand chunk
 constexpr int kStages = 3;
 constexpr int kAccCols = 64;                  // tail accumulator: half a tile
 constexpr int kAccLd = kAccCols + 1;          // odd stride: conflict-free row reads
-constexpr int kECap = 7680;                   // I-block tail postings staged per chunk
 constexpr uint32_t kTmemCols = 256;
 constexpr int kComputeBar = 1;
-constexpr int kBatch = 8;                     // J postings per thread per load batch
+constexpr int kBatch = 4;                     // J postings per thread per load batch
 constexpr int kEpiCols = kAccCols / (kCW / 4);  // tile columns per thread per half (16)
 
 struct SmemM {
@@ -68,10 +67,9 @@ struct SmemM {
 __host__ __device__ constexpr size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
 struct Layout {
-  size_t acc, hnj, bars, tmem, abort, gf, eu, bloom, warm, gs, er, total;
+  size_t acc, hnj, bars, tmem, abort, hash, eu, gs, er, total;
   __host__ __device__ constexpr Layout()
-      : acc(0), hnj(0), bars(0), tmem(0), abort(0), gf(0), eu(0), bloom(0), warm(0), gs(0), er(0),
-        total(0) {
+      : acc(0), hnj(0), bars(0), tmem(0), abort(0), hash(0), eu(0), gs(0), er(0), total(0) {
     size_t o = (size_t)kStages * 2 * kTileBytes;
     acc = o;
     o += (size_t)kBlockRows * kAccLd * 4;
@@ -83,18 +81,14 @@ struct Layout {
     o = tmem + 16;
     abort = o;
     o += 16;
-    gf = align_up(o, 16);
-    o = gf + (size_t)kECap * 4;
+    hash = align_up(o, 16);
+    o = hash + (size_t)kBuckets * 16;
     eu = align_up(o, 16);
-    o = eu + (size_t)kECap * 4;
-    bloom = align_up(o, 16);
-    o = bloom + (size_t)kBloomWords * 4;
-    warm = align_up(o, 16);
-    o = warm + (size_t)kWarm * 2;
+    o = eu + (size_t)kChunkPostings * 4;
     gs = align_up(o, 16);
-    o = gs + ((size_t)kECap + 8) * 2;
+    o = gs + ((size_t)kChunkGroups + 8) * 2;
     er = align_up(o, 16);
-    o = er + (size_t)kECap;
+    o = er + (size_t)kChunkPostings;
     total = align_up(o, 16);
   }
 };
@@ -116,13 +110,11 @@ __device__ __forceinline__ SmemM carve(uint8_t* raw) {
   s.drain = b + 2 * kStages + 4;
   s.tmem_base = reinterpret_cast<uint32_t*>(base + kLayout.tmem);
   s.abort = reinterpret_cast<int*>(base + kLayout.abort);
-  s.ts.gf = reinterpret_cast<uint32_t*>(base + kLayout.gf);
+  s.ts.hash = reinterpret_cast<uint4*>(base + kLayout.hash);
   s.ts.eu = reinterpret_cast<float*>(base + kLayout.eu);
-  s.ts.bloom = reinterpret_cast<uint32_t*>(base + kLayout.bloom);
-  s.ts.warm = reinterpret_cast<uint16_t*>(base + kLayout.warm);
   s.ts.gs = reinterpret_cast<uint16_t*>(base + kLayout.gs);
   s.ts.er = base + kLayout.er;
-  s.ts.ecap = kECap;
+  s.ts.ecap = kChunkPostings;
   return s;
 }
 
@@ -131,7 +123,7 @@ __device__ __forceinline__ bool wait_or_abort(uint64_t* bar, uint32_t parity,
                                               const volatile int* abort) {
   for (uint32_t i = 0; i < kMaxPolls; ++i) {
     if (mbar_try_wait(bar, parity)) return true;
-    if ((i & 31u) == 31u && *abort) return false;
+    if (*abort) return false;
   }
   return false;
 }
@@ -185,6 +177,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_tiles_mma(const TileArgs A, con
       bool ok = true;
       for (int u = blockIdx.x; ok && u < A.nunits; u += gridDim.x) {
         const int4 U = A.units[u];
+        if (U.y >= U.z) continue;
         for (int J = U.y; ok && J < U.z; ++J) {
           for (int kc = 0; kc < M.nkc; ++kc, ++it) {
             const uint32_t s = it % kStages, round = it / kStages;
@@ -216,6 +209,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_tiles_mma(const TileArgs A, con
       bool ok = true;
       for (int u = blockIdx.x; ok && u < A.nunits; u += gridDim.x) {
         const int4 U = A.units[u];
+        if (U.y >= U.z) continue;
         for (int J = U.y; ok && J < U.z; ++J, ++tt) {
           const uint32_t b = tt & 1u, tround = tt >> 1;
           if (!wait_or_abort(&S.tempty[b], (tround & 1u) ^ 1u, abort)) {
@@ -253,28 +247,22 @@ __global__ void __launch_bounds__(kThreads, 1) k_tiles_mma(const TileArgs A, con
     __syncwarp();
   } else {
     // ---------------------------------------------- tail + epilogue warps
-    // The J postings of the next half-tile are loaded into registers before
-    // the current epilogue, so their latency hides behind it.
     const int ctid = threadIdx.x - 64;
     const int q = warp & 3;             // tensor-memory lane quarter of this warp
     const int colq = (warp - 2) >> 2;   // which kEpiCols of each 64 columns
     const int row = 32 * q + lane;
     uint32_t tt = 0;
     bool ok = true;
-    TailBatch<kBatch> B;
-    if ((int)blockIdx.x < A.nunits) {
-      const int J0 = A.units[blockIdx.x].y;
-      tail_prefetch(A, B, A.hptrJ[2 * J0], A.hptrJ[2 * J0 + 1], ctid, kCT);
-    }
     for (int u = blockIdx.x; ok && u < A.nunits; u += gridDim.x) {
       const int4 U = A.units[u];
+      if (U.y >= U.z) continue;
       const int I = U.x;
       const int64_t row0 = (int64_t)I * kBlockRows;
       const int rowsI = (int)(A.nI - row0 < kBlockRows ? A.nI - row0 : kBlockRows);
       named_bar(kComputeBar, kCT);
-      const int nch = tail_nchunks(A, I, kECap);
+      const int nch = tail_nchunks(A, I);
       TailI T{};
-      if (nch == 1) T = stage_tail_chunk<kCT, kComputeBar>(A, S.ts, I, 0, 1, ctid);
+      if (nch == 1) T = stage_tail_chunk<kCT, kComputeBar>(A, S.ts, I, 0, ctid);
       const float hn_r = row < rowsI ? A.hnormI[row0 + row] : 0.0f;
       for (int J = U.y; ok && J < U.z; ++J, ++tt) {
         const uint32_t b = tt & 1u, tround = tt >> 1;
@@ -287,14 +275,18 @@ __global__ void __launch_bounds__(kThreads, 1) k_tiles_mma(const TileArgs A, con
           S.hnj[ctid] =
               ctid < colsJ ? __double2float_ru(A.eps_head * (double)A.hnormJ[col0 + ctid]) : 0.0f;
         for (int h = 0; h < 2; ++h) {
-          // ---- tail of this half-tile (its first batch is already in B)
-          if (nch == 1) {
-            tail_postings_pre<kBatch>(A, S.ts, T, B, S.acc, kAccLd, h * kAccCols, ctid, kCT);
-          } else {
-            for (int c = 0; c < nch; ++c) {
-              const TailI Tc = stage_tail_chunk<kCT, kComputeBar>(A, S.ts, I, c, nch, ctid);
-              tail_postings_pre<kBatch>(A, S.ts, Tc, B, S.acc, kAccLd, h * kAccCols, ctid, kCT);
-              named_bar(kComputeBar, kCT);  // staging rewritten by the next chunk
+          // ---- tail of this half-tile
+          {
+            const int64_t k0 = A.hptrJ[2 * J + h], k1 = A.hptrJ[2 * J + h + 1];
+            if (nch == 1) {
+              tail_postings<kBatch>(A, S.ts, T, k0, k1, S.acc, kAccLd, h * kAccCols, ctid, kCT);
+            } else {
+              for (int c = 0; c < nch; ++c) {
+                const TailI Tc = stage_tail_chunk<kCT, kComputeBar>(A, S.ts, I, c, ctid);
+                tail_postings<kBatch>(A, S.ts, Tc, k0, k1, S.acc, kAccLd, h * kAccCols, ctid,
+                                      kCT);
+                named_bar(kComputeBar, kCT);  // staging rewritten by the next chunk
+              }
             }
           }
           named_bar(kComputeBar, kCT);
@@ -306,20 +298,6 @@ __global__ void __launch_bounds__(kThreads, 1) k_tiles_mma(const TileArgs A, con
               break;
             }
             tc_fence_after();
-          }
-          // ---- prefetch the next half-tile's postings
-          {
-            int nJ = -1, nh = 0;
-            if (h == 0) {
-              nJ = J;
-              nh = 1;
-            } else if (J + 1 < U.z) {
-              nJ = J + 1;
-            } else if (u + (int)gridDim.x < A.nunits) {
-              nJ = A.units[u + gridDim.x].y;
-            }
-            if (nJ >= 0)
-              tail_prefetch(A, B, A.hptrJ[2 * nJ + nh], A.hptrJ[2 * nJ + nh + 1], ctid, kCT);
           }
           // ---- epilogue: head (tensor memory) + tail (shared) vs t - eps
           const int cbase = h * kAccCols + colq * kEpiCols;  // first tile column of this thread

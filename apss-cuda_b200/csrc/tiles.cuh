@@ -23,6 +23,8 @@ struct TileArgs {
   const int64_t* gptrI;     // groups of each I block
   const uint32_t* gstartI;  // entries of each group
   const uint32_t* gfeatI;   // feature of each group
+  const int64_t* chunk_ptrI;  // staging-chunk boundaries of each I block
+  const int64_t* chunk_gI;
   const uint32_t* bilI_f;
   const uint8_t* bilI_r;
   const float* bilI_u;
