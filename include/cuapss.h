@@ -164,6 +164,17 @@ cuapss_status cuapss_build_index(cuapss_ctx* ctx, const cuapss_csr* x,
 cuapss_status cuapss_feature_remap(cuapss_ctx* ctx, const cuapss_csr* x,
                                    int32_t* perm, int32_t* counts);
 
+/* The same remap as cuapss_feature_remap, with no device allocation: for
+ * callers whose device memory belongs to another allocator or whose latency
+ * path forbids cudaMalloc/cudaFree. x, perm and counts must be device
+ * pointers on ctx's device (x->on_device = 1); all other memory is a fixed
+ * ~1.6 MB file-scope device array, so d <= 65536 (larger d: CUAPSS_EINVAL).
+ * The first call on a device looks up that array's address and should come
+ * before any stream capture. Calls that overlap on the GPU share the array
+ * and race: serialise them. No counterpart in the reference. */
+cuapss_status cuapss_feature_remap_noalloc(cuapss_ctx* ctx, const cuapss_csr* x,
+                                           int32_t* perm, int32_t* counts);
+
 #ifdef __cplusplus
 }
 #endif
