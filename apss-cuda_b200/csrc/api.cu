@@ -159,7 +159,6 @@ cuapss_status join_device(cuapss_ctx* ctx, const DevCsr& a, const DevCsr* b, flo
   }
   cudaEventRecord(ctx->ev[1], st);
   // ---- pair tiles ----
-  const double u = std::ldexp(1.0, -24);
   const double nrm2 = nrm_a * nrm_b;
   TileArgs ta{};
   ta.headI32 = SA.head32;
@@ -185,21 +184,9 @@ cuapss_status join_device(cuapss_ctx* ctx, const DevCsr& a, const DevCsr* b, flo
   ta.p = SA.p;
   ta.self = self ? 1 : 0;
   ta.t = t;
-  // FP32 head chain + fixed-point tail (2^-30 grid, exact sums) + final add:
-  // |s~ - s| <= (K + 3) u ||a|| ||b|| + K 2^-31, K = shared features
   if (nrm2 >= 1.9) return CUAPSS_EINVAL;  // fixed-point tail needs ~unit norms
   if (d - SA.p > (int64_t)(1u << 20) - 2) return CUAPSS_EINVAL;  // 20-bit tail feature keys
-  ta.eps_c1 = (u * nrm2 + std::ldexp(1.0, -31)) * 1.001;
-  ta.eps_c0 = 3.0 * u * nrm2 * 1.001 + 1e-10;
-  ta.eps_head = 0.0;
-  if (mixed) {
-    // BF16 inputs: each factor rounded to 8 significant bits (relative
-    // 2^-8), products exact in FP32; tensor-core accumulation over p/16
-    // steps bounded by 2^-20 relative per step.
-    ta.eps_head = (std::ldexp(1.0, -7) + std::ldexp(1.0, -16)) +
-                  (SA.p / 16.0 + 2.0) * std::ldexp(1.0, -20) * (1.0 + std::ldexp(1.0, -7));
-    ta.eps_head *= 1.001;
-  }
+  set_tile_margins(ta, nrm2, mixed);
   // ---- units: I block x J range; an I block's J range is cut into chunks
   // of about equal cost (about 16 units per CTA), heavier blocks get shorter
   // ranges. CTAs take units round-robin (mixed kernel) or from a counter.
@@ -425,6 +412,8 @@ cuapss_status cuapss_destroy(cuapss_ctx* c) {
   if (!c) return CUAPSS_OK;
   cudaSetDevice(c->device);
   cudaStreamSynchronize(c->stream);
+  if (c->batch_exec) cudaGraphExecDestroy(c->batch_exec);
+  if (c->batch_graph) cudaGraphDestroy(c->batch_graph);
   c->ws.release();
   for (auto& e : c->ev)
     if (e) cudaEventDestroy(e);

@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 
+#include <map>
 #include <string>
 
 #include "common.cuh"
@@ -18,6 +19,11 @@ struct cuapss_ctx {
   cuapss::Workspace ws;
   cudaEvent_t ev[6] = {};
   int64_t cand_cap = 0;
+  // batched joins: the captured tile launches (updated in place when the
+  // next batch has the same launch topology) and the tuner's choices
+  cudaGraph_t batch_graph = nullptr;
+  cudaGraphExec_t batch_exec = nullptr;
+  std::map<uint64_t, int> tuned_p;
 };
 
 namespace cuapss {

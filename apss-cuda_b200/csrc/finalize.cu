@@ -79,13 +79,14 @@ __global__ void __launch_bounds__(kThreads) k_finalize(const FinalizeArgs A) {
     double eps = A.eps_c1 * K + A.eps_c0;
     if (A.eps_head > 0.0) eps += A.eps_head * (double)A.hnormI[inew] * (double)A.hnormJ[jnew];
     const double lo = (double)st - eps, hi = (double)st + eps;
-    if (hi < (double)A.t) continue;
+    const double t = A.t_blk ? (double)A.t_blk[inew / kBlockRows] : (double)A.t;
+    if (hi < t) continue;
     const int32_t oi = A.rowpermI[inew], oj = A.rowpermJ[jnew];
     const int64_t ai = A.rpI[oi], an = A.rpI[oi + 1] - ai;
     const int64_t bj = A.rpJ[oj], bn = A.rpJ[oj + 1] - bj;
     float sim;
     bool in;
-    if (lo >= (double)A.t) {
+    if (lo >= t) {
       in = true;
       sim = dot2_fp32(A.colI + ai, A.valI + ai, an, A.colJ + bj, A.valJ + bj, bn);
     } else {
@@ -93,11 +94,17 @@ __global__ void __launch_bounds__(kThreads) k_finalize(const FinalizeArgs A) {
       // FP64 in the oracle's order: the self-join oracle walks the lower id's
       // row, which for a product of two exact factors gives the same sums.
       const double s64 = dot_fp64(A.colI + ai, A.valI + ai, an, A.colJ + bj, A.valJ + bj, bn);
-      in = s64 >= (double)A.t;
+      in = s64 >= t;
       sim = (float)s64;
     }
     if (!in) continue;
-    uint64_t a = (uint64_t)oi, b = (uint64_t)oj;
+    int32_t ri = oi, rj = oj;
+    if (A.slot_row) {
+      ri = A.slot_row[oi];
+      rj = A.slot_row[oj];
+      if (ri < 0 || rj < 0) continue;  // padding rows (empty) of a batched layout
+    }
+    uint64_t a = (uint64_t)ri, b = (uint64_t)rj;
     if (A.self && a > b) {
       const uint64_t tmp = a;
       a = b;

@@ -41,6 +41,12 @@ struct Rng {
   }
 };
 
+// Seed of the per-row streams: the table seed itself, or (stream != 0) an
+// independent stream over the same feature permutation.
+inline uint64_t row_seed(const cuapss_synth_params* p) {
+  return p->stream == 0 ? p->seed : mix64(p->seed ^ mix64(0x53545245414dull + p->stream));
+}
+
 struct Tables {
   std::vector<double> cdf;     // cdf[r], r = 0..d-1 (rank r+1)
   std::vector<int32_t> guide;  // guide[b] = smallest r with cdf[r] > b/G
@@ -95,7 +101,7 @@ inline int32_t zipf_rank(const Tables& t, double u) {
 }
 
 int64_t orig_nnz(const cuapss_synth_params* p, int64_t row) {
-  Rng rng(p->seed, kTagNnz, (uint64_t)row);
+  Rng rng(row_seed(p), kTagNnz, (uint64_t)row);
   const double mu = std::log(p->nnz_mean) - 0.5 * p->nnz_sigma * p->nnz_sigma;
   const double x = std::exp(mu + p->nnz_sigma * rng.normal());
   int64_t k = (int64_t)std::llround(x);
@@ -108,7 +114,7 @@ int64_t orig_nnz(const cuapss_synth_params* p, int64_t row) {
 // Returns base row (>= 0) if `row` is a planted duplicate, else -1.
 int64_t dup_base(const cuapss_synth_params* p, int64_t row) {
   if (row <= 0 || p->dup_frac <= 0) return -1;
-  Rng rng(p->seed, kTagDup, (uint64_t)row);
+  Rng rng(row_seed(p), kTagDup, (uint64_t)row);
   if (rng.uniform() >= p->dup_frac) return -1;
   int64_t b = (int64_t)(rng.uniform() * (double)row);
   if (b >= row) b = row - 1;
@@ -133,7 +139,7 @@ struct Scratch {
 void orig_row(const cuapss_synth_params* p, const Tables& t, int64_t row,
               Scratch* s) {
   const int64_t k = orig_nnz(p, row);
-  Rng rng(p->seed, kTagRow, (uint64_t)row);
+  Rng rng(row_seed(p), kTagRow, (uint64_t)row);
   int64_t cap = 16;
   while (cap < 2 * k) cap <<= 1;
   s->slots.assign(cap, -1);
@@ -232,7 +238,7 @@ extern "C" int cuapss_synth_fill(const cuapss_synth_params* p,
           bad = 1;
           continue;
         }
-        Rng rng(p->seed, kTagDupRow, (uint64_t)row);
+        Rng rng(row_seed(p), kTagDupRow, (uint64_t)row);
         s.idx.resize(k);
         for (int64_t e = 0; e < k; ++e) s.idx[e] = (int32_t)e;
         // partial Fisher-Yates: the first k-keep slots are the dropped ones

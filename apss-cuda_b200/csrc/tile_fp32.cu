@@ -24,6 +24,8 @@
 // counter by persistent CTAs.
 #include <cuda_runtime.h>
 
+#include <mutex>
+
 #include <climits>
 
 #include "ptx.cuh"
@@ -166,7 +168,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_tiles_fp32(const TileArgs A) {
         const int colsJ = (int)(A.nJ - col0 < kBlockRows ? A.nJ - col0 : kBlockRows);
         const bool diag = A.self && (I == J);
         const int kmax = min(A.blkmaxI[I], A.blkmaxJ[J]);
-        const float t_lo = __double2float_rd((double)A.t - (A.eps_c1 * kmax + A.eps_c0));
+        const float t_lo = __double2float_rd((double)(A.t_blk ? A.t_blk[I] : A.t) -
+                                             (A.eps_c1 * kmax + A.eps_c0));
         unsigned long long pass = 0ull;
 #pragma unroll
         for (int i = 0; i < 8; ++i) {
@@ -234,13 +237,23 @@ int tiles_fp32_max_grid() {
   return sms;
 }
 
+// Opts the kernel into its dynamic shared memory once per device (outside
+// any stream capture when called ahead of it).
+cuapss_status tiles_fp32_init() {
+  static std::mutex mu;
+  static uint64_t done = 0;  // bit per device
+  int dev = 0;
+  CU_TRY(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lk(mu);
+  if (dev < 64 && ((done >> dev) & 1ull)) return CUAPSS_OK;
+  CU_TRY(cudaFuncSetAttribute(k_tiles_fp32, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)kSmemBytes));
+  if (dev < 64) done |= 1ull << dev;
+  return CUAPSS_OK;
+}
+
 cuapss_status launch_tiles_fp32(const TileArgs& a, int grid, cudaStream_t st) {
-  static bool attr_set = false;
-  if (!attr_set) {
-    CU_TRY(cudaFuncSetAttribute(k_tiles_fp32, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)kSmemBytes));
-    attr_set = true;
-  }
+  ST_TRY(tiles_fp32_init());
   if (a.p % kKC != 0) return CUAPSS_EINVAL;
   k_tiles_fp32<<<grid, kThreads, kSmemBytes, st>>>(a);
   LAUNCH_CHECK();

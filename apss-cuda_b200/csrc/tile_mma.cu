@@ -29,6 +29,8 @@
 // MMAs, frees tensor memory and returns.
 #include <cuda_runtime.h>
 
+#include <mutex>
+
 #include "ptx.cuh"
 #include "tail.cuh"
 #include "tiles.cuh"
@@ -270,7 +272,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_tiles_mma(const TileArgs A, con
         const int colsJ = (int)(A.nJ - col0 < kBlockRows ? A.nJ - col0 : kBlockRows);
         const bool diag = A.self && (I == J);
         const int kmax = min(A.blkmaxI[I], A.blkmaxJ[J]);
-        const float t_lo = __double2float_rd((double)A.t - (A.eps_c1 * kmax + A.eps_c0));
+        const float t_lo = __double2float_rd((double)(A.t_blk ? A.t_blk[I] : A.t) -
+                                             (A.eps_c1 * kmax + A.eps_c0));
         if (ctid < kBlockRows)
           S.hnj[ctid] =
               ctid < colsJ ? __double2float_ru(A.eps_head * (double)A.hnormJ[col0 + ctid]) : 0.0f;
@@ -364,14 +367,24 @@ __global__ void __launch_bounds__(kThreads, 1) k_tiles_mma(const TileArgs A, con
 
 }  // namespace
 
+// Opts the kernel into its dynamic shared memory once per device (outside
+// any stream capture when called ahead of it).
+cuapss_status tiles_mma_init() {
+  static std::mutex mu;
+  static uint64_t done = 0;  // bit per device
+  int dev = 0;
+  CU_TRY(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lk(mu);
+  if (dev < 64 && ((done >> dev) & 1ull)) return CUAPSS_OK;
+  CU_TRY(cudaFuncSetAttribute(k_tiles_mma, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)kSmemBytes));
+  if (dev < 64) done |= 1ull << dev;
+  return CUAPSS_OK;
+}
+
 cuapss_status launch_tiles_mma(const TileArgs& a, const void* headI16, const void* headJ16,
                                int p, int grid, cudaStream_t st) {
-  static bool attr_set = false;
-  if (!attr_set) {
-    CU_TRY(cudaFuncSetAttribute(k_tiles_mma, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)kSmemBytes));
-    attr_set = true;
-  }
+  ST_TRY(tiles_mma_init());
   if (p <= 0 || p % kKC != 0) return CUAPSS_EINVAL;
   MmaArgs m;
   m.headI16 = static_cast<const uint8_t*>(headI16);

@@ -1,6 +1,7 @@
 // Launch interfaces of the pair-tile kernels and the finalize stage.
 #pragma once
 
+#include <cmath>
 #include <cstdint>
 
 #include "common.cuh"
@@ -40,6 +41,7 @@ struct TileArgs {
   int p;
   int self;
   float t;
+  const float* t_blk;  // per I block threshold (batched instances), or null: t
   double eps_c1;  // FP32 error margin of a tile: eps_c1 * min(maxnnz_I, maxnnz_J) + eps_c0
   double eps_c0;
   double eps_head;  // tensor-core path: extra margin per unit of ||a_h|| ||b_h||
@@ -53,9 +55,28 @@ struct TileArgs {
   int* err;
 };
 
+// Error margins of the tile decision for rows of norm <= sqrt(nrm2) and head
+// width ta.p. FP32 head chain + fixed-point tail (2^-30 grid, exact sums) +
+// final add: |s~ - s| <= (K + 3) u ||a|| ||b|| + K 2^-31, K = shared
+// features. Tensor-core head (mixed): each BF16 factor is rounded to 8
+// significant bits (relative 2^-8), products are exact in FP32, and the
+// accumulation over p/16 MMA steps is bounded by 2^-20 relative per step.
+inline void set_tile_margins(TileArgs& ta, double nrm2, bool mixed) {
+  const double u = std::ldexp(1.0, -24);
+  ta.eps_c1 = (u * nrm2 + std::ldexp(1.0, -31)) * 1.001;
+  ta.eps_c0 = 3.0 * u * nrm2 * 1.001 + 1e-10;
+  ta.eps_head = 0.0;
+  if (mixed) {
+    ta.eps_head = (std::ldexp(1.0, -7) + std::ldexp(1.0, -16)) +
+                  (ta.p / 16.0 + 2.0) * std::ldexp(1.0, -20) * (1.0 + std::ldexp(1.0, -7));
+    ta.eps_head *= 1.001;
+  }
+}
+
 // Plain FP32 hybrid tile kernel (head: FP32 forward-list dot on TMA-staged
 // row tiles; tail: inverted-list scan into shared-memory accumulators).
 cuapss_status launch_tiles_fp32(const TileArgs& a, int grid, cudaStream_t st);
+cuapss_status tiles_fp32_init();
 int tiles_fp32_max_grid();
 
 // Mixed-precision tile kernel (BF16 head on tcgen05 tensor cores, FP32 tail).
@@ -64,6 +85,10 @@ int tiles_fp32_max_grid();
 cuapss_status launch_tiles_mma(const TileArgs& a, const void* headI16, const void* headJ16,
                                int p, int grid, cudaStream_t st);
 size_t tiles_mma_smem_bytes();
+cuapss_status tiles_mma_init();
+
+// Kernel attributes of the tile kernel of a precision, on the current device.
+inline cuapss_status tiles_init(bool mixed) { return mixed ? tiles_mma_init() : tiles_fp32_init(); }
 
 struct FinalizeArgs {
   const uint64_t* cand_key;
@@ -82,6 +107,8 @@ struct FinalizeArgs {
   const int32_t* colJ;
   const float* valJ;
   float t;
+  const float* t_blk;       // per I row block threshold, or null: t
+  const int32_t* slot_row;  // side row -> caller's row (-1: padding), or null: rowperm
   double eps_c1;
   double eps_c0;
   double eps_head;

@@ -99,6 +99,7 @@ _lib = None
 EXPORTED = [
     "cuapss_default_opts", "cuapss_status_string", "cuapss_abi_version", "cuapss_create",
     "cuapss_destroy", "cuapss_run", "cuapss_join", "cuapss_build_index", "cuapss_feature_remap",
+    "cuapss_batch_run",
 ]
 
 
@@ -130,6 +131,9 @@ def lib():
         L.cuapss_build_index.restype = ctypes.c_int
         L.cuapss_feature_remap.argtypes = [_P, ctypes.POINTER(CsrDesc), _P, _P]
         L.cuapss_feature_remap.restype = ctypes.c_int
+        L.cuapss_batch_run.argtypes = [_P, ctypes.POINTER(CsrDesc), ctypes.c_int32, _P, _P,
+                                       ctypes.POINTER(PairsDesc), ctypes.POINTER(Stats), _P]
+        L.cuapss_batch_run.restype = ctypes.c_int
         _lib = L
     return _lib
 
@@ -239,6 +243,58 @@ class Context:
         db, kb = _desc(b)
         return self._pairs_call(lib().cuapss_join,
                                 (ctypes.byref(da), ctypes.byref(db), ctypes.c_float(t)), capacity)
+
+    def _batch_args(self, x, inst_ptr, t):
+        d, keep = _desc(x)
+        ip = np.ascontiguousarray(inst_ptr, dtype=np.int64)
+        tq = np.ascontiguousarray(t, dtype=np.float32)
+        if ip.ndim != 1 or tq.shape != (ip.size - 1,):
+            raise ValueError("inst_ptr has k+1 entries and t has k")
+        return d, keep, ip, tq
+
+    def batch_run(self, x, inst_ptr, t, capacity: int = 1 << 16):
+        """Batched self-joins of the row ranges [inst_ptr[q], inst_ptr[q+1])
+        of x, instance q at threshold t[q]: (i, j, sim) in x's rows, sorted.
+        The head width used per size bucket is left in self.last_bucket_p."""
+        d, keep, ip, tq = self._batch_args(x, inst_ptr, t)
+        cap = max(int(capacity), 1)
+        bp = np.zeros(3, np.int32)
+        while True:
+            oi = np.empty(cap, np.int32)
+            oj = np.empty(cap, np.int32)
+            os_ = np.empty(cap, np.float32)
+            pr = PairsDesc(oi.ctypes.data, oj.ctypes.data, os_.ctypes.data, cap, 0, 0)
+            st = Stats()
+            s = lib().cuapss_batch_run(self._h, ctypes.byref(d), int(tq.size), ip.ctypes.data,
+                                       tq.ctypes.data, ctypes.byref(pr), ctypes.byref(st),
+                                       bp.ctypes.data)
+            if s == EOVERFLOW:
+                cap = int(pr.count)
+                continue
+            _check(s, "cuapss_batch_run")
+            self.last_stats = st.as_dict()
+            self.last_bucket_p = bp.copy()
+            n = int(pr.count)
+            return oi[:n].copy(), oj[:n].copy(), os_[:n].copy()
+
+    def batch_run_device(self, x, inst_ptr, t, out: dict):
+        """batch_run with x a dict of CUDA tensors and the pairs written to
+        CUDA tensors out = {"i", "j", "sim"}; returns the pair count (raises
+        CuapssError(EOVERFLOW) with self.required set if short)."""
+        d, keep, ip, tq = self._batch_args(x, inst_ptr, t)
+        cap = int(out["i"].numel())
+        pr = PairsDesc(out["i"].data_ptr(), out["j"].data_ptr(), out["sim"].data_ptr(), cap, 0, 1)
+        st = Stats()
+        bp = np.zeros(3, np.int32)
+        s = lib().cuapss_batch_run(self._h, ctypes.byref(d), int(tq.size), ip.ctypes.data,
+                                   tq.ctypes.data, ctypes.byref(pr), ctypes.byref(st),
+                                   bp.ctypes.data)
+        self.last_stats = st.as_dict()
+        self.last_bucket_p = bp.copy()
+        if s == EOVERFLOW:
+            self.required = int(pr.count)
+        _check(s, "cuapss_batch_run")
+        return int(pr.count)
 
     def build_index(self, x: Csr, p: int):
         """Reference-semantics tail index: (dim_ptr[d+1], rows, vals)."""

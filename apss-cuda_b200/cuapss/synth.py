@@ -31,6 +31,7 @@ class _Params(ctypes.Structure):
         ("dup_scale_hi", ctypes.c_double),
         ("seed", ctypes.c_uint64),
         ("row_offset", ctypes.c_int64),
+        ("stream", ctypes.c_uint64),
     ]
 
 
@@ -50,6 +51,7 @@ class SynthConfig:
     dup_scale_lo: float = 0.9
     dup_scale_hi: float = 1.1
     seed: int = 0
+    stream: int = 0
 
     def replace(self, **kw) -> "SynthConfig":
         return dataclasses.replace(self, **kw)
@@ -101,7 +103,7 @@ def lib():
 def _params(cfg: SynthConfig, row_offset: int = 0) -> _Params:
     return _Params(cfg.n, cfg.d, cfg.nnz_mean, cfg.nnz_sigma, cfg.nnz_max, cfg.zipf_s,
                    cfg.tf_p, cfg.dup_frac, cfg.dup_drop, cfg.dup_scale_lo, cfg.dup_scale_hi,
-                   cfg.seed, row_offset)
+                   cfg.seed, row_offset, cfg.stream)
 
 
 class Csr:
@@ -174,3 +176,49 @@ def generate(cfg: SynthConfig | str, row_offset: int = 0, **overrides) -> Csr:
 
 def host_threads() -> int:
     return int(lib().cuapss_synth_threads())
+
+
+# The batched workload: 4,096 independent instances, n log-uniform in
+# [64, 20,000], thresholds uniform in [0.6, 0.95], rows of "batch_instance".
+BATCH = dict(k=4096, n_lo=64, n_hi=20_000, t_lo=0.6, t_hi=0.95)
+
+
+def generate_batch(k: int = BATCH["k"], n_lo: int = BATCH["n_lo"], n_hi: int = BATCH["n_hi"],
+                   t_lo: float = BATCH["t_lo"], t_hi: float = BATCH["t_hi"], seed: int = 0,
+                   cfg: SynthConfig | str = "batch_instance"):
+    """k independent instances stacked as row ranges of one CSR.
+
+    Instance q has n_q ~ logU[n_lo, n_hi] rows drawn from its own row stream
+    (same feature permutation, so the same vocabulary) and threshold
+    t_q ~ U[t_lo, t_hi]. Returns (Csr, inst_ptr int64[k+1], t float32[k])."""
+    if isinstance(cfg, str):
+        cfg = CONFIGS[cfg]
+    rng = np.random.default_rng(seed)
+    ns = np.floor(np.exp(rng.uniform(np.log(n_lo), np.log(n_hi + 1), size=k))).astype(np.int64)
+    ns = np.clip(ns, n_lo, n_hi)
+    ts = rng.uniform(t_lo, t_hi, size=k).astype(np.float32)
+    inst_ptr = np.zeros(k + 1, np.int64)
+    np.cumsum(ns, out=inst_ptr[1:])
+    L = lib()
+    rp = np.zeros(int(inst_ptr[-1]) + 1, np.int64)
+    params = []
+    for q in range(k):
+        c = cfg.replace(n=int(ns[q]), seed=seed, stream=q + 1)
+        pq = _params(c, 0)
+        part = np.zeros(int(ns[q]) + 1, np.int64)
+        if L.cuapss_synth_rowptr(ctypes.byref(pq), part.ctypes.data) != 0:
+            raise ValueError(f"bad generator parameters {c}")
+        a = int(inst_ptr[q])
+        rp[a + 1:a + 1 + int(ns[q])] = part[1:] + rp[a]
+        params.append(pq)
+    nnz = int(rp[-1])
+    col = np.empty(max(nnz, 1), np.int32)
+    val = np.empty(max(nnz, 1), np.float32)
+    for q in range(k):
+        a, b = int(inst_ptr[q]), int(inst_ptr[q + 1])
+        e0 = int(rp[a])
+        local = rp[a:b + 1] - e0
+        if L.cuapss_synth_fill(ctypes.byref(params[q]), local.ctypes.data,
+                               col[e0:].ctypes.data, val[e0:].ctypes.data) != 0:
+            raise ValueError("generator failed")
+    return Csr(rp, col[:nnz], val[:nnz], cfg.d), inst_ptr, ts

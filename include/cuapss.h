@@ -143,6 +143,28 @@ cuapss_status cuapss_join(cuapss_ctx* ctx, const cuapss_csr* a,
                           const cuapss_csr* b, float t, cuapss_pairs* out,
                           cuapss_stats* stats);
 
+/* Size buckets of the batched self-join (instance rows n):
+ * bucket 0: n <= 1024, bucket 1: n <= 8192, bucket 2: larger. */
+#define CUAPSS_BATCH_BUCKETS 3
+
+/* Batched self-joins of k independent instances: instance q is the row range
+ * [inst_ptr[q], inst_ptr[q+1]) of `x` (inst_ptr[0] = 0, inst_ptr[k] = x->n,
+ * non-decreasing; host array) with its own threshold t[q] (host array, each
+ * > 0). Pairs never cross instances. Output as cuapss_run: (i, j, sim) in
+ * x's row numbering, i < j, sorted by (i, j), so grouped by instance. All
+ * instances share the feature remap; each size bucket gets its own head
+ * width p (opts.head_width if set, else the context's autotuner, which times
+ * candidate widths on a sample of the bucket the first time it meets a bucket
+ * with those nnz statistics and keeps the winner). The tile launches of all
+ * buckets run as one CUDA graph launch. bucket_p (may be NULL) receives the
+ * width used per bucket (0: bucket empty). The reference runs its 8
+ * partition self-joins one after another, two launches and host syncs each
+ * (similarity_search.cu:2650-2993); it has no batched form. */
+cuapss_status cuapss_batch_run(cuapss_ctx* ctx, const cuapss_csr* x, int32_t k,
+                               const int64_t* inst_ptr, const float* t,
+                               cuapss_pairs* out, cuapss_stats* stats,
+                               int32_t* bucket_p);
+
 /* Inverted index of the tail features, reference semantics: for every
  * feature f with f >= p (on the caller's ids, no remap), the rows that
  * contain f and their values, lists sorted by row. dim_ptr has d+1 entries

@@ -40,6 +40,10 @@ typedef struct {
   uint64_t seed;
   int64_t row_offset;  /* generate rows [row_offset, row_offset + n) of the
                           stream defined by seed (for appends / shards) */
+  uint64_t stream;     /* 0: the rows of seed's stream; else an independent
+                          row stream over the same feature permutation (one
+                          per instance of a batch: same vocabulary, own rows
+                          and own planted duplicates) */
 } cuapss_synth_params;
 
 /* Fill rowptr[0..n] (rowptr[0] = 0). Returns 0, or -1 on bad parameters. */

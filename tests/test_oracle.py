@@ -115,3 +115,21 @@ def test_cpu_hybrid_counts_match_oracle():
         want = len(oracle.apss(x, t)[0])
         got, _, _ = oracle.cpu_hybrid(x, t, 64, 0, x.n)
         assert abs(got - want) <= max(2, want // 1000)
+
+
+def test_batch_generator_layout():
+    x, ip, t = synth.generate_batch(k=50, n_lo=64, n_hi=2000, seed=9)
+    assert ip[0] == 0 and ip[-1] == x.n and np.all(np.diff(ip) >= 64)
+    assert np.all(np.diff(ip) <= 2000) and t.shape == (50,)
+    assert np.all((t >= 0.6) & (t <= 0.95))
+    nrm = np.sqrt(np.add.reduceat(x.val.astype(np.float64) ** 2, x.rowptr[:-1]))
+    assert np.allclose(nrm, 1.0, atol=1e-5)
+    # instance rows come from independent streams over one vocabulary: the
+    # same seed gives the same batch, stream 0 is the plain stream
+    x2, ip2, t2 = synth.generate_batch(k=50, n_lo=64, n_hi=2000, seed=9)
+    np.testing.assert_array_equal(x.col, x2.col)
+    a = synth.generate("batch_instance", n=100)
+    b = synth.generate("batch_instance", n=100, stream=0)
+    np.testing.assert_array_equal(a.col, b.col)
+    c = synth.generate("batch_instance", n=100, stream=3)
+    assert not np.array_equal(a.col[:50], c.col[:50])
