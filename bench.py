@@ -18,6 +18,8 @@ through the C ABI with pinned host buffers: the CSR upload and the pair-list
 download are inside the timed region.
 
   python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+  python bench.py --workload mixed_1m   # n = d = 1,000,000, Zipf(1.2), mean nnz 120
+  python bench.py --workload batch      # 4,096 uneven instances, per-instance t
 Multi-GPU (torchrun): every rank runs its own replica of the workload (the
 path has no cross-GPU exchange); value sums the ranks, time is the max.
 """
@@ -200,6 +202,221 @@ def run_reference(args, rank, world):
     print(json.dumps(line))
 
 
+def run_batch(args, rank, world, local):
+    """--workload batch: 4,096 independent instances (n log-uniform in
+    [64, 20,000], d = 30,000, thresholds uniform in [0.6, 0.95]) in one
+    cuapss_batch_run per step. value = sum of n_q(n_q-1)/2 per step / device
+    time. Compared with launching the plain FP32 path once per instance."""
+    import numpy as np
+    import torch
+
+    import cuapss
+    from cuapss import synth
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    x, ip, tq = synth.generate_batch(k=args.k, seed=0)
+    ns = np.diff(ip)
+    pairs_per_step = float((ns * (ns - 1) // 2).sum())
+    prec = cuapss.PREC_MIXED if args.precision == "mixed" else cuapss.PREC_FP32
+    dev = {"rowptr": torch.from_numpy(x.rowptr).cuda(), "col": torch.from_numpy(x.col).cuda(),
+           "val": torch.from_numpy(x.val).cuda(), "d": x.d}
+    stream = torch.cuda.Stream()
+    ctx = cuapss.Context(device=local, precision=prec, head_width=args.head,
+                         stream=stream.cuda_stream)
+
+    def alloc(c):
+        return {"i": torch.empty(c, dtype=torch.int32, device="cuda"),
+                "j": torch.empty(c, dtype=torch.int32, device="cuda"),
+                "sim": torch.empty(c, dtype=torch.float32, device="cuda")}
+
+    cap = 1 << 22
+    out = alloc(cap)
+
+    def step():
+        nonlocal out, cap
+        while True:
+            try:
+                return ctx.batch_run_device(dev, ip, tq, out)
+            except cuapss.CuapssError as e:
+                if e.status != cuapss.EOVERFLOW:
+                    raise
+                cap = ctx.required + 1024
+                out = alloc(cap)
+
+    for _ in range(max(args.warmup, 1)):  # the first call runs the autotuner
+        npairs = step()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    stats = []
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with Clocks(local) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            npairs = step()
+            stats.append(dict(ctx.last_stats))
+        e1.record(stream)
+        torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    ms = e0.elapsed_time(e1) / args.steps
+    if dist:
+        tms = torch.tensor([ms], device="cuda")
+        dist.all_reduce(tms, op=dist.ReduceOp.MAX)
+        ms = float(tms.item())
+    value = world * pairs_per_step / (ms / 1e3)
+    clocks = clk.summary()
+    bucket_p = [int(v) for v in ctx.last_bucket_p]
+
+    e2e = None
+    if not args.no_e2e:
+        hp = {"rowptr": torch.from_numpy(x.rowptr).pin_memory(),
+              "col": torch.from_numpy(x.col).pin_memory(),
+              "val": torch.from_numpy(x.val).pin_memory()}
+        hcap = max(npairs, 1)
+        ho = {"i": torch.empty(hcap, dtype=torch.int32).pin_memory(),
+              "j": torch.empty(hcap, dtype=torch.int32).pin_memory(),
+              "sim": torch.empty(hcap, dtype=torch.float32).pin_memory()}
+        desc = cuapss.CsrDesc(x.n, x.d, x.nnz, hp["rowptr"].data_ptr(), hp["col"].data_ptr(),
+                              hp["val"].data_ptr(), 0)
+        ipc = np.ascontiguousarray(ip, np.int64)
+        tqc = np.ascontiguousarray(tq, np.float32)
+        L = cuapss.lib()
+
+        def hstep():
+            pr = cuapss.PairsDesc(ho["i"].data_ptr(), ho["j"].data_ptr(), ho["sim"].data_ptr(),
+                                  hcap, 0, 0)
+            s = L.cuapss_batch_run(ctx._h, ctypes.byref(desc), int(len(tqc)), ipc.ctypes.data,
+                                   tqc.ctypes.data, ctypes.byref(pr), None, None)
+            if s != cuapss.OK:
+                raise cuapss.CuapssError(s, "cuapss_batch_run (host buffers)")
+            return int(pr.count)
+
+        hstep()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        f0 = torch.cuda.Event(enable_timing=True)
+        f1 = torch.cuda.Event(enable_timing=True)
+        f0.record(stream)
+        for _ in range(args.steps):
+            hn = hstep()
+        f1.record(stream)
+        torch.cuda.synchronize()
+        ems = f0.elapsed_time(f1) / args.steps
+        if dist:
+            tms = torch.tensor([ems], device="cuda")
+            dist.all_reduce(tms, op=dist.ReduceOp.MAX)
+            ems = float(tms.item())
+        e2e = {"value": world * pairs_per_step / (ems / 1e3), "unit": "pairs/s",
+               "ms_per_step": ems,
+               "h2d_bytes_per_step": int(x.rowptr.nbytes + x.col.nbytes + x.val.nbytes +
+                                         ipc.nbytes + tqc.nbytes),
+               "d2h_bytes_per_step": int(hn * 12)}
+
+    hbm, bf16, src = peaks()
+    tile_ms = sum(s["ms_tiles"] for s in stats) / len(stats)
+    s0 = stats[-1]
+    tiles = int(s0["tiles"])
+    if prec == cuapss.PREC_MIXED:
+        # head GEMM flops of the tiles actually run: 2 * 128 * 128 * p per
+        # tile, p of the bucket that owns the most tiles (stats.head_width)
+        flops = 2.0 * 128 * 128 * int(s0["head_width"]) * tiles
+        achieved = flops / (tile_ms / 1e3) / 1e12
+        roofline = {"bound": "tensor", "achieved": achieved, "peak": bf16, "unit": "TFLOP/s",
+                    "frac": achieved / bf16, "traffic": None, "peak_source": src,
+                    "kernel": "k_tiles_mma", "kernel_ms": tile_ms, "algorithmic_flops": flops,
+                    "note": "tensor-core head flops of the 128x128 tiles over the tile-graph "
+                            "time (one launch per size bucket)"}
+    else:
+        alg_bytes = 8.0 * s0["tail_products"] + 12.0 * s0["candidates"]
+        achieved_gbs = alg_bytes / (tile_ms / 1e3) / 1e9
+        roofline = {"bound": "hbm", "achieved": achieved_gbs, "peak": hbm, "unit": "GB/s",
+                    "frac": achieved_gbs / hbm, "traffic": None, "peak_source": src,
+                    "kernel": "k_tiles_fp32", "kernel_ms": tile_ms}
+
+    # ---- comparison: the plain FP32 path launched once per instance
+    per_inst = None
+    if not args.no_plain:
+        pctx = cuapss.Context(device=local, precision=cuapss.PREC_FP32, stream=stream.cuda_stream)
+        insts = []
+        for q in range(len(tq)):
+            lo, hi = int(ip[q]), int(ip[q + 1])
+            e_0, e_1 = int(x.rowptr[lo]), int(x.rowptr[hi])
+            insts.append((q, {"rowptr": torch.from_numpy(x.rowptr[lo:hi + 1] - e_0).cuda(),
+                              "col": dev["col"][e_0:e_1], "val": dev["val"][e_0:e_1],
+                              "d": x.d}))
+        pout = alloc(max(cap, 1 << 20))
+        for q, d in insts[:16]:
+            pctx.run_device(d, float(tq[q]), pout)
+        torch.cuda.synchronize()
+        g0 = torch.cuda.Event(enable_timing=True)
+        g1 = torch.cuda.Event(enable_timing=True)
+        g0.record(stream)
+        tot = 0
+        for q, d in insts:
+            tot += pctx.run_device(d, float(tq[q]), pout)
+        g1.record(stream)
+        torch.cuda.synchronize()
+        pms = g0.elapsed_time(g1)
+        per_inst = {"value": world * pairs_per_step / (pms / 1e3), "unit": "pairs/s",
+                    "ms_per_step": pms, "pairs_found": tot,
+                    "same_pair_count_as_batch": tot == npairs,
+                    "batch_over_per_instance": pms / ms,
+                    "note": "cuapss_run (plain FP32) once per instance, inputs resident"}
+        pctx.close()
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32" if prec == cuapss.PREC_FP32 else "bf16 head + f32 tail + f64 band",
+        "data": "synthetic (seeded generator, independent row stream per instance)",
+        "config": {"workload": "batch", "instances": int(len(tq)), "rows": x.n, "d": x.d,
+                   "nnz": x.nnz, "n_range": [int(ns.min()), int(ns.max())],
+                   "t_range": [float(tq.min()), float(tq.max())], "precision": args.precision,
+                   "bucket_head_width": bucket_p,
+                   "l2": "inputs larger than L2 (3.3 GB CSR)",
+                   "parallelism": f"replicas x{world}"},
+        "pairs_found": npairs, "candidates": s0["candidates"], "rescored": s0["rescored"],
+        "tiles": tiles,
+        "stage_ms": {k: sum(s[k] for s in stats) / len(stats)
+                     for k in ("ms_preprocess", "ms_tiles", "ms_finalize", "ms_total")},
+        "gpu_launches": int(sum(s["launches"] for s in stats)),
+        "clocks": clocks, "roofline": roofline, "e2e": e2e, "per_instance_fp32": per_inst,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu:
+        from oracle import oracle
+        threads = oracle.max_threads()
+        rng = np.random.default_rng(7)
+        done_pairs, secs, used = 0.0, 0.0, 0
+        for q in rng.permutation(len(tq)):
+            lo, hi = int(ip[q]), int(ip[q + 1])
+            _, sp, sq = oracle.cpu_hybrid(x.rows(lo, hi), float(tq[q]), 128, 0, hi - lo, threads)
+            secs += sp + sq
+            done_pairs += (hi - lo) * (hi - lo - 1) / 2
+            used += 1
+            if secs > 12.0:
+                break
+        line["cpu_baseline"] = {"value": done_pairs / secs, "unit": "pairs/s", "cores": threads,
+                                "kind": "port",
+                                "sample": f"{used} random instances of the batch, each a full "
+                                          f"self-join ({done_pairs:.3g} pairs, {secs:.1f} s)"}
+    if rank == 0:
+        print(json.dumps(line))
+    ctx.close()
+    if dist:
+        dist.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -215,10 +432,17 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--ref-index-rows", type=int, default=100_000)
     ap.add_argument("--ref-step-s", type=float, default=8.0)
+    ap.add_argument("--workload", default=WORKLOAD, choices=["plain_800k", "mixed_1m", "batch"],
+                    help="plain_800k (default); mixed_1m: n = d = 1M; batch: 4,096 instances")
+    ap.add_argument("--k", type=int, default=4096, help="instances of the batch workload")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.workload == "batch" and args.impl == "cuapss":
+        run_batch(args, rank, world, local)
+        return
+    workload = args.workload if args.workload != "batch" else WORKLOAD
     if args.impl == "reference":
         run_reference(args, rank, world)
         return
@@ -237,7 +461,7 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device("cuda", local))
-    x = synth.generate(WORKLOAD, n=args.n) if args.n else synth.generate(WORKLOAD)
+    x = synth.generate(workload, n=args.n) if args.n else synth.generate(workload)
     prec = cuapss.PREC_MIXED if args.precision == "mixed" else cuapss.PREC_FP32
     dev = {"rowptr": torch.from_numpy(x.rowptr).cuda(), "col": torch.from_numpy(x.col).cuda(),
            "val": torch.from_numpy(x.val).cuda(), "d": x.d}
@@ -390,7 +614,7 @@ def main():
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32" if prec == cuapss.PREC_FP32 else "bf16 head + f32 tail + f64 band",
         "data": "synthetic (seeded generator, reference corpus not distributed)",
-        "config": {"workload": WORKLOAD, "n": x.n, "d": x.d, "nnz": x.nnz, "t": args.t,
+        "config": {"workload": workload, "n": x.n, "d": x.d, "nnz": x.nnz, "t": args.t,
                    "precision": args.precision, "head_width": p,
                    "l2": "inputs larger than L2 (CSR + head block > 126 MB)",
                    "parallelism": f"replicas x{world}"},
