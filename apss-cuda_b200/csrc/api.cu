@@ -44,7 +44,7 @@ int choose_head_width(int precision, int64_t n, int64_t d, int64_t nnz) {
   (void)nnz;
   // measured on the lognormal/Zipf workloads: the tensor-core head is cheap,
   // so a wide head shrinks the sparse tail; the FP32 head pays per feature
-  int p = precision == CUAPSS_PREC_MIXED ? 1024 : 128;
+  int p = precision == CUAPSS_PREC_MIXED ? 1024 : 64;
   const int64_t cap = ((d + 31) / 32) * 32;
   if (p > cap) p = (int)cap;
   return p;
@@ -166,13 +166,9 @@ cuapss_status join_device(cuapss_ctx* ctx, const DevCsr& a, const DevCsr* b, flo
   ta.nbI = SA.nb;
   ta.blkmaxI = SA.blk_maxnnz;
   ta.hnormI = SA.hnorm;
-  ta.gptrI = SA.gptr;
-  ta.gstartI = SA.gstart;
-  ta.gfeatI = SA.gfeat;
-  ta.chunk_ptrI = SA.chunk_ptr;
-  ta.chunk_gI = SA.chunk_g;
-  ta.bilI_f = SA.bil_f;
-  ta.bilI_r = SA.bil_r;
+  ta.bptrI = SA.bptr;
+  ta.bilI_key = SA.bil_key;
+  ta.bilI_len = SA.bil_len;
   ta.bilI_u = SA.bil_u;
   ta.headJ32 = SJ->head32;
   ta.nJ = SJ->n;

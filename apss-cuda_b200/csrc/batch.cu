@@ -189,13 +189,9 @@ cuapss_status prepare_bucket(cuapss_ctx* ctx, const BatchIn& in, Bucket& b, int 
   ta.nbI = ta.nbJ = s.nb;
   ta.blkmaxI = ta.blkmaxJ = s.blk_maxnnz;
   ta.hnormI = ta.hnormJ = s.hnorm;
-  ta.gptrI = s.gptr;
-  ta.gstartI = s.gstart;
-  ta.gfeatI = s.gfeat;
-  ta.chunk_ptrI = s.chunk_ptr;
-  ta.chunk_gI = s.chunk_g;
-  ta.bilI_f = s.bil_f;
-  ta.bilI_r = s.bil_r;
+  ta.bptrI = s.bptr;
+  ta.bilI_key = s.bil_key;
+  ta.bilI_len = s.bil_len;
   ta.bilI_u = s.bil_u;
   ta.hptrJ = s.hptr;
   ta.bilJ_rec = s.bil_rec;

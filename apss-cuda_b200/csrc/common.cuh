@@ -55,8 +55,10 @@ enum : int {
 constexpr int kBlockRows = 128;  // rows per row block (tile edge)
 // Tail staging capacity of the tile kernels: a block's feature groups are
 // staged in shared memory in chunks of at most this many groups / postings.
-constexpr int kChunkGroups = 4096;
-constexpr int kChunkPostings = 8192;
+// Tail postings of a row block are bucketed by the low kTailBucketBits bits
+// of the tail feature (see tail.cuh).
+constexpr int kTailBucketBits = 12;
+constexpr uint32_t kTailBuckets = 1u << kTailBucketBits;
 
 inline int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
 

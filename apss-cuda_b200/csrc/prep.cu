@@ -226,9 +226,25 @@ __global__ void k_head16_scatter(const int64_t* __restrict__ rp2, const int32_t*
   }
 }
 
+// Block-local lists are ordered by (bucket = f mod 2^12, tag = f >> 12):
+// the fb-bit feature rotated so that its low 12 bits lead (a bijection, so
+// equal features stay contiguous).
+__device__ __forceinline__ uint32_t tail_rot(uint32_t f, int fb) {
+  return fb > kTailBucketBits
+             ? ((f & (kTailBuckets - 1u)) << (fb - kTailBucketBits)) | (f >> kTailBucketBits)
+             : f;
+}
+__device__ __forceinline__ uint32_t tail_unrot(uint32_t k, int fb) {
+  return fb > kTailBucketBits
+             ? ((k & ((1u << (fb - kTailBucketBits)) - 1u)) << kTailBucketBits) |
+                   (k >> (fb - kTailBucketBits))
+             : k;
+}
+
 // One warp per new row: tail entries in row order, sort keys for the
-// block-local lists (block, feature) and, optionally, the global lists
-// (feature, row); posting counts per tail feature.
+// block-local lists (block, bucket, tag) and the half-block lists
+// (half-block, feature) and, optionally, the global lists (feature, row);
+// posting counts per tail feature.
 __global__ void k_tail_entries(const int64_t* __restrict__ rp2, const int32_t* __restrict__ col2,
                                const float* __restrict__ val2, const int32_t* __restrict__ hlen,
                                const int64_t* __restrict__ tptr, int64_t n, int p, int rbits,
@@ -250,7 +266,7 @@ __global__ void k_tail_entries(const int64_t* __restrict__ rp2, const int32_t* _
       tk[t] = (uint32_t)k;
       tr[t] = (uint8_t)(r % kBlockRows);
       tu[t] = val2[k];
-      bkeys[t] = (blk << fb) | (uint64_t)f;
+      bkeys[t] = (blk << fb) | (uint64_t)tail_rot((uint32_t)f, fb);
       bvals[t] = (uint32_t)t;
       hkeys[t] = (hblk << fb) | (uint64_t)f;
       hvals[t] = (uint32_t)t;
@@ -263,19 +279,29 @@ __global__ void k_tail_entries(const int64_t* __restrict__ rp2, const int32_t* _
   }
 }
 
+// I-side postings in (block, bucket, tag, row) order: key {bucket << 15 |
+// tag << 7 | row in block}, value, and at the first posting of each
+// feature's run the run's length (a run is one feature of one block, at most
+// kBlockRows postings; 0 elsewhere).
 __global__ void k_bil_fill(const uint64_t* __restrict__ keys, const uint32_t* __restrict__ vals,
                            const uint8_t* __restrict__ tr, const float* __restrict__ tu, int64_t T,
-                           uint64_t fmask, uint32_t* __restrict__ bil_f, uint8_t* __restrict__ bil_r,
-                           float* __restrict__ bil_u, uint32_t* __restrict__ flags) {
+                           int fb, uint32_t* __restrict__ bil_key, float* __restrict__ bil_u,
+                           uint8_t* __restrict__ bil_len) {
+  const uint64_t fmask = (1ull << fb) - 1ull;
   for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < T;
        k += (int64_t)gridDim.x * blockDim.x) {
     const uint64_t key = keys[k];
     const uint32_t t = vals[k];
-    const uint32_t f = (uint32_t)(key & fmask);
-    bil_f[k] = f;
-    bil_r[k] = tr[t];
+    const uint32_t f = tail_unrot((uint32_t)(key & fmask), fb);
+    bil_key[k] = ((f & (kTailBuckets - 1u)) << 15) | ((f >> kTailBucketBits) << 7) | (uint32_t)tr[t];
     bil_u[k] = tu[t];
-    flags[k] = (k == 0 || keys[k - 1] != key) ? 1u : 0u;
+    int len = 0;
+    if (k == 0 || keys[k - 1] != key) {
+      int64_t m = k + 1;
+      while (m < T && m - k < kBlockRows && keys[m] == key) ++m;
+      len = (int)(m - k);
+    }
+    bil_len[k] = (uint8_t)len;
   }
 }
 
@@ -298,57 +324,11 @@ __global__ void k_half_ptrs(const int64_t* __restrict__ tptr, int64_t n, int nh,
     hptr[h] = tptr[min(n, h * (kBlockRows / 2))];
 }
 
-// Staging chunks of each block's feature groups: a chunk holds at most
-// kChunkGroups groups and kChunkPostings postings (one thread per block).
-template <bool FILL>
-__global__ void k_chunk_bounds(const int64_t* __restrict__ gptr, const uint32_t* __restrict__ gstart,
-                               int nb, int64_t* __restrict__ count,
-                               const int64_t* __restrict__ cptr, int64_t* __restrict__ bnd) {
-  for (int64_t b = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; b < nb;
-       b += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t g0 = gptr[b], g1 = gptr[b + 1];
-    int64_t s = g0, k = 0;
-    if (FILL) bnd[cptr[b]] = g0;
-    while (s < g1) {
-      const int64_t e1 = min(g1, s + (int64_t)kChunkGroups);
-      const uint32_t lim = gstart[s] + (uint32_t)kChunkPostings;
-      int64_t lo = s + 1, hi = e1;  // largest e in [s+1, e1] with gstart[e] <= lim
-      while (lo < hi) {
-        const int64_t mid = (lo + hi + 1) >> 1;
-        if (gstart[mid] <= lim) lo = mid;
-        else hi = mid - 1;
-      }
-      s = lo;
-      ++k;
-      if (FILL) bnd[cptr[b] + k] = s;
-    }
-    if (!FILL) count[b] = k + 1;  // chunk boundaries of block b (an empty block: 1)
-  }
-}
-
-__global__ void k_group_starts(const uint32_t* __restrict__ flags, const uint32_t* __restrict__ gidx,
-                               const uint32_t* __restrict__ bil_f, int64_t T,
-                               uint32_t* __restrict__ gstart, uint32_t* __restrict__ gfeat) {
-  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k <= T;
-       k += (int64_t)gridDim.x * blockDim.x) {
-    if (k == T) {
-      gstart[gidx[T]] = (uint32_t)T;
-    } else if (flags[k]) {
-      gstart[gidx[k]] = (uint32_t)k;
-      gfeat[gidx[k]] = bil_f[k];
-    }
-  }
-}
-
-__global__ void k_block_ptrs(const int64_t* __restrict__ tptr, const uint32_t* __restrict__ gidx,
-                             int64_t n, int nb, int64_t* __restrict__ bptr,
-                             int64_t* __restrict__ gptr) {
+__global__ void k_block_ptrs(const int64_t* __restrict__ tptr, int64_t n, int nb,
+                             int64_t* __restrict__ bptr) {
   for (int64_t b = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; b <= nb;
-       b += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t e = tptr[min(n, b * kBlockRows)];
-    bptr[b] = e;
-    gptr[b] = gidx[e];
-  }
+       b += (int64_t)gridDim.x * blockDim.x)
+    bptr[b] = tptr[min(n, b * kBlockRows)];
 }
 
 __global__ void k_csc_fill(const uint64_t* __restrict__ keys, const uint32_t* __restrict__ vals,
@@ -524,17 +504,18 @@ cuapss_status build_side(Side& s, const PrepOptions& o, const int32_t* perm, Wor
                                                                       s.hlen, n, nkc, s.head16);
     LAUNCH_CHECK();
   }
-  // ---- tail: entries in row order, block-local inverted lists, groups ----
+  // ---- tail: entries in row order, block-local inverted lists ----
   CU_TRY(cudaMemcpyAsync(&s.ntail, s.tptr + n, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
   CU_TRY(cudaStreamSynchronize(st));
   const int64_t T = s.ntail;
   if (T >= (int64_t)UINT32_MAX - 1) return CUAPSS_EINVAL;
   const int64_t nf = std::max<int64_t>(d - p, 0);
-  if (nf >= (1 << 24)) return CUAPSS_EINVAL;  // packed postings hold 24-bit features
+  // I-side keys hold an 8-bit tag above the 12-bit bucket: tail features < 2^20
+  if (nf > (1 << 20)) return CUAPSS_EINVAL;
   const int fb = std::max(1, bits_for((uint64_t)nf));
   const int bb = std::max(1, bits_for((uint64_t)nb));
   uint64_t *ckeys = nullptr, *bkeys = nullptr, *hkeys = nullptr;
-  uint32_t *cvals = nullptr, *bvals = nullptr, *hvals = nullptr, *flags = nullptr;
+  uint32_t *cvals = nullptr, *bvals = nullptr, *hvals = nullptr;
   int32_t* ccount = nullptr;
   ST_TRY(ws.get(t + "tk", (size_t)T, &s.tk));
   ST_TRY(ws.get(t + "tr", (size_t)T, &s.tr));
@@ -553,16 +534,14 @@ cuapss_status build_side(Side& s, const PrepOptions& o, const int32_t* perm, Wor
       s.rp2, s.col2, s.val2, s.hlen, s.tptr, n, p, rbits, fb, s.tk, s.tr, s.tu, ckeys, cvals,
       bkeys, bvals, hkeys, hvals, ccount);
   LAUNCH_CHECK();
-  // block-local inverted lists: stable sort by (block, feature) keeps rows
-  // ascending inside a feature; groups come from a scan of head flags
+  // block-local inverted lists: stable sort by (block, bucket, tag) keeps
+  // rows ascending inside a feature
   ST_TRY(radix_sort_pairs(bkeys, bvals, T, bb + fb, ws, t + "bil", st));
-  ST_TRY(ws.get(t + "bil_f", (size_t)T, &s.bil_f));
-  ST_TRY(ws.get(t + "bil_r", (size_t)T, &s.bil_r));
+  ST_TRY(ws.get(t + "bil_key", (size_t)T, &s.bil_key));
   ST_TRY(ws.get(t + "bil_u", (size_t)T, &s.bil_u));
-  ST_TRY(ws.get(t + "gflags", (size_t)T + 1, &flags));
-  k_bil_fill<<<grid_for(T, kThreads), kThreads, 0, st>>>(bkeys, bvals, s.tr, s.tu, T,
-                                                        (1ull << fb) - 1, s.bil_f, s.bil_r,
-                                                        s.bil_u, flags);
+  ST_TRY(ws.get(t + "bil_len", (size_t)T, &s.bil_len));
+  k_bil_fill<<<grid_for(T, kThreads), kThreads, 0, st>>>(bkeys, bvals, s.tr, s.tu, T, fb,
+                                                        s.bil_key, s.bil_u, s.bil_len);
   LAUNCH_CHECK();
   // J-side postings: per 64-row half-block, sorted by feature, packed
   {
@@ -577,41 +556,9 @@ cuapss_status build_side(Side& s, const PrepOptions& o, const int32_t* perm, Wor
     k_half_ptrs<<<grid_for(nh + 1, kThreads), kThreads, 0, st>>>(s.tptr, n, nh, s.hptr);
     LAUNCH_CHECK();
   }
-  uint32_t* gidx = nullptr;
-  ST_TRY(ws.get(t + "gidx", (size_t)T + 1, &gidx));
-  ST_TRY(exclusive_scan<uint32_t>(flags, gidx, T, gidx + T, ws, t + "gidx", st));
-  uint32_t G32 = 0;
-  CU_TRY(cudaMemcpyAsync(&G32, gidx + T, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
-  CU_TRY(cudaStreamSynchronize(st));
-  s.ngroups = G32;
-  ST_TRY(ws.get(t + "gstart", (size_t)s.ngroups + 1, &s.gstart));
-  ST_TRY(ws.get(t + "gfeat", (size_t)s.ngroups + 1, &s.gfeat));
   ST_TRY(ws.get(t + "bptr", (size_t)nb + 1, &s.bptr));
-  ST_TRY(ws.get(t + "gptr", (size_t)nb + 1, &s.gptr));
-  k_group_starts<<<grid_for(T + 1, kThreads), kThreads, 0, st>>>(flags, gidx, s.bil_f, T,
-                                                                   s.gstart, s.gfeat);
+  k_block_ptrs<<<grid_for(nb + 1, kThreads), kThreads, 0, st>>>(s.tptr, n, nb, s.bptr);
   LAUNCH_CHECK();
-  k_block_ptrs<<<grid_for(nb + 1, kThreads), kThreads, 0, st>>>(s.tptr, gidx, n, nb, s.bptr,
-                                                                 s.gptr);
-  LAUNCH_CHECK();
-  // ---- staging chunks of every block ----
-  {
-    int64_t* ccnt = nullptr;
-    ST_TRY(ws.get(t + "chunk_cnt", (size_t)nb + 1, &ccnt));
-    ST_TRY(ws.get(t + "chunk_ptr", (size_t)nb + 1, &s.chunk_ptr));
-    k_chunk_bounds<false><<<grid_for(nb, 128), 128, 0, st>>>(s.gptr, s.gstart, nb, ccnt, nullptr,
-                                                             nullptr);
-    LAUNCH_CHECK();
-    ST_TRY(exclusive_scan<int64_t>(ccnt, s.chunk_ptr, nb, s.chunk_ptr + nb, ws, t + "chunk", st));
-    int64_t total = 0;
-    CU_TRY(cudaMemcpyAsync(&total, s.chunk_ptr + nb, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
-    CU_TRY(cudaStreamSynchronize(st));
-    ST_TRY(ws.get(t + "chunk_g", (size_t)std::max<int64_t>(total, 1), &s.chunk_g));
-    k_chunk_bounds<true><<<grid_for(nb, 128), 128, 0, st>>>(s.gptr, s.gstart, nb, nullptr,
-                                                            s.chunk_ptr, s.chunk_g);
-    LAUNCH_CHECK();
-    s.nchunk_bounds = total;
-  }
   // ---- global inverted lists (feature, row), on request ----
   if (o.want_csc) {
     uint32_t* entpos = nullptr;
@@ -636,19 +583,13 @@ cuapss_status build_side(Side& s, const PrepOptions& o, const int32_t* perm, Wor
   unsigned long long hred[2] = {0, 0};
   CU_TRY(cudaMemcpyAsync(hred, red, sizeof(hred), cudaMemcpyDeviceToHost, st));
   s.h_bptr.resize(nb + 1);
-  s.h_gptr.resize(nb + 1);
   CU_TRY(cudaMemcpyAsync(s.h_bptr.data(), s.bptr, sizeof(int64_t) * (nb + 1),
-                         cudaMemcpyDeviceToHost, st));
-  CU_TRY(cudaMemcpyAsync(s.h_gptr.data(), s.gptr, sizeof(int64_t) * (nb + 1),
                          cudaMemcpyDeviceToHost, st));
   CU_TRY(cudaStreamSynchronize(st));
   s.tail_products = (int64_t)hred[0];
   s.max_block_tail = 0;
-  s.max_block_groups = 0;
-  for (int b = 0; b < nb; ++b) {
+  for (int b = 0; b < nb; ++b)
     s.max_block_tail = std::max<int64_t>(s.max_block_tail, s.h_bptr[b + 1] - s.h_bptr[b]);
-    s.max_block_groups = std::max<int64_t>(s.max_block_groups, s.h_gptr[b + 1] - s.h_gptr[b]);
-  }
   return CUAPSS_OK;
 }
 

@@ -19,18 +19,15 @@
 //                             request)
 //   tptr      int64[n+1]      tail entries of each row, in row order
 //   bptr      int64[nb+1]     tail entries of each row block
-//   bil_f/bil_r/bil_u         block-local inverted lists: the tail postings
-//                             of each row block sorted by (feature, row):
-//                             feature - p, row inside the block, value
+//   bil_key/bil_u/bil_len     block-local inverted lists: the tail postings
+//                             of each row block sorted by (bucket = f mod
+//                             2^12, tag = f >> 12, row), f = feature - p:
+//                             key {bucket << 15 | tag << 7 | row in block},
+//                             value, and the length of each feature's run at
+//                             its first posting
 //   bil_rec   uint2[T]        the same postings per 64-row half-block, sorted by
 //                             feature, packed {feature << 8 | row, value}
 //   hptr      int64[2nb+1]    postings of each half-block
-//   gstart    uint32[G+1]     feature groups: entries [gstart[g], gstart[g+1])
-//                             of the BIL share one feature
-//   gfeat     uint32[G]       feature of each group
-//   gptr      int64[nb+1]     groups of each row block
-//   chunk_ptr/chunk_g         staging chunks of each block (at most
-//                             kChunkGroups groups, kChunkPostings postings)
 #pragma once
 
 #include <cuda_bf16.h>
@@ -67,24 +64,15 @@ struct Side {
   uint8_t* tr = nullptr;          // row-order tail entries: row in block, value
   float* tu = nullptr;
   int64_t* bptr = nullptr;
-  uint32_t* bil_f = nullptr;
-  uint8_t* bil_r = nullptr;
+  uint32_t* bil_key = nullptr;    // I-side postings {bucket << 15 | tag << 7 | row}
   float* bil_u = nullptr;
+  uint8_t* bil_len = nullptr;     // run length at a feature's first posting, else 0
   uint2* bil_rec = nullptr;       // J-side postings per 64-row half-block, sorted by
                                   // feature: {feature << 8 | row in block, value bits}
   int64_t* hptr = nullptr;        // [2 nb + 1] postings of each half-block
-  uint32_t* gstart = nullptr;
-  uint32_t* gfeat = nullptr;      // feature of each group
-  int64_t* chunk_ptr = nullptr;   // [nb+1] staging-chunk boundaries of each block
-  int64_t* chunk_g = nullptr;     // boundaries (group indices), nchunks+1 per block
-  int64_t nchunk_bounds = 0;
-  int64_t* gptr = nullptr;
-  int64_t ngroups = 0;
-  int64_t max_block_groups = 0;
   int64_t ntail = 0;
   int64_t max_block_tail = 0;
   std::vector<int64_t> h_bptr;    // host copy of bptr (unit scheduling)
-  std::vector<int64_t> h_gptr;    // host copy of gptr
   int64_t tail_products = 0;      // sum over tail lists of L(L-1)/2
   double nrm_max = 1.0;           // largest row norm (FP64)
 };

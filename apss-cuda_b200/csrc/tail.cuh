@@ -2,20 +2,22 @@
 // part of the hybrid similarity.
 //
 // I side (the rows of a tile; fixed for a unit of work): the block-local
-// inverted list of the 128-row block, grouped by feature, is staged in
-// shared memory: the postings (row in block, value), the first posting of
-// every group, and a hash of the group features. The hash is an array of
-// 16-byte buckets of 4 packed slots {(feature + 1) << 12 | group}; a lookup
-// reads one bucket (one 128-bit shared load) and compares four keys, and
-// only a full bucket sends it to the next one. A block larger than the
-// staging capacity (kGroupCap groups, ecap postings) is staged in chunks of
-// consecutive groups, whose boundaries are computed once per block by the
-// preprocessing.
+// inverted list of the 128-row block is staged in shared memory as a
+// bucketed posting list. The preprocessing sorts the block's tail postings
+// by (bucket = f mod 2^12, tag = f >> 12, row), f the tail feature, so a
+// staged posting is {tag << 7 | row} (16 bits), its value (FP32) and, at the
+// first posting of each feature's run, the run length (8 bits); a table of
+// 4097 bucket offsets (16 bits each) delimits the buckets. Staging is a
+// straight copy plus the offsets: no hashing, no atomics. A block with more
+// than kStagePostings postings is staged in consecutive chunks of
+// kStagePostings postings (any cut is valid: every chunk adds the products
+// of its own postings; a run cut by a chunk boundary is re-measured).
 //
 // J side (the columns; one per tile): the tail postings of each 64-row
 // half-block sorted by feature, packed as {feature << 8 | column, value}.
-// Each posting (c, f, v) whose feature the I block contains adds u * v for
-// every I posting (r, u) of that group into the shared-memory accumulator
+// A J posting (c, f, v) reads the two offsets of bucket f mod 2^12 and walks
+// that bucket run by run (tags ascend) to the run with tag f >> 12; each of
+// its postings (r, u) adds u * v into the shared-memory accumulator
 // acc[r][c] with an integer atomic on a fixed-point grid of 2^-30: FP32
 // products are rounded to the grid and the integer sums are exact in any
 // order, so the tail is deterministic and its error is the product rounding
@@ -32,31 +34,39 @@
 
 namespace cuapss {
 
-constexpr int kGroupCap = kChunkGroups;  // groups per staged chunk (12-bit slot value)
-static_assert(kGroupCap <= 4096, "slot value is 12 bits");
-constexpr int kBuckets = 2048;        // hash buckets of 4 slots (load <= 1/2)
-constexpr uint32_t kMaxTailFeature = (1u << 20) - 2;  // 20-bit slot key = feature + 1
+constexpr int kStagePostings = 12800;  // postings per staged chunk (16-bit offsets)
+static_assert(kStagePostings < 65536, "bucket offsets are 16 bits");
+constexpr uint32_t kMaxTailFeature = (1u << 20) - 1;  // 8-bit tag above 12-bit bucket
 constexpr float kTailScale = 1073741824.0f;              // 2^30
 constexpr float kTailUnscale = 9.313225746154785e-10f;   // 2^-30
 
-__device__ __forceinline__ int tail_fixed(float prod) { return __float2int_rn(prod * kTailScale); }
+constexpr size_t kTailOffBytes = ((size_t)(kTailBuckets + 1) * 2 + 15) / 16 * 16;
+// Shared memory of the staged I postings.
+constexpr size_t kTailStageBytes = kTailOffBytes + (size_t)kStagePostings * 7;
 
-__device__ __forceinline__ uint32_t tail_bucket(uint32_t f) {
-  return (f * 2654435761u) >> (32 - 11);  // 11 bits: kBuckets
-}
+__device__ __forceinline__ int tail_fixed(float prod) { return __float2int_rn(prod * kTailScale); }
 
 // Shared-memory staging buffers of the I side.
 struct TailStage {
-  uint4* hash;     // [kBuckets] 4 packed slots each, 0 = empty
-  uint16_t* gs;    // [kGroupCap + 1] first posting of each group (chunk relative)
-  uint8_t* er;     // [ecap] posting: row in block
-  float* eu;       // [ecap] posting: value
-  int ecap;
+  uint16_t* boff;  // [kTailBuckets + 1] first posting of each bucket
+  float* eu;       // [kStagePostings] posting: value
+  uint16_t* et;    // [kStagePostings] posting: tag << 7 | row in block
+  uint8_t* en;     // [kStagePostings] run length at a run's first posting
 };
+
+// Carves a TailStage out of kTailStageBytes of 16-byte aligned shared memory.
+__device__ __forceinline__ TailStage tail_stage_at(uint8_t* base) {
+  TailStage t;
+  t.boff = reinterpret_cast<uint16_t*>(base);
+  t.eu = reinterpret_cast<float*>(base + kTailOffBytes);
+  t.et = reinterpret_cast<uint16_t*>(base + kTailOffBytes + (size_t)kStagePostings * 4);
+  t.en = base + kTailOffBytes + (size_t)kStagePostings * 6;
+  return t;
+}
 
 // The staged chunk.
 struct TailI {
-  int G;
+  int P;     // postings staged
   bool any;
 };
 
@@ -66,10 +76,10 @@ __device__ __forceinline__ void tail_sync() {
   else named_bar(BAR, NT);
 }
 
-// Chunks of I block I: chunk c holds the groups
-// [chunk_gI[chunk_ptrI[I] + c], chunk_gI[chunk_ptrI[I] + c + 1]).
+// Chunks of I block I (at least one, possibly empty).
 __device__ __forceinline__ int tail_nchunks(const TileArgs& A, int I) {
-  return (int)(A.chunk_ptrI[I + 1] - A.chunk_ptrI[I]) - 1;
+  const int64_t T = A.bptrI[I + 1] - A.bptrI[I];
+  return T <= kStagePostings ? 1 : (int)((T + kStagePostings - 1) / kStagePostings);
 }
 
 // Stage chunk c of block I. All NT tail threads (ltid = index among them)
@@ -77,72 +87,67 @@ __device__ __forceinline__ int tail_nchunks(const TileArgs& A, int I) {
 template <int NT, int BAR>
 __device__ __forceinline__ TailI stage_tail_chunk(const TileArgs& A, const TailStage& S, int I,
                                                   int c, int ltid) {
-  const int64_t cb = A.chunk_ptrI[I] + c;
-  const int64_t ga = A.chunk_gI[cb], gb = A.chunk_gI[cb + 1];
-  const uint32_t e0 = A.gstartI[ga];
-  const uint32_t e1 = A.gstartI[gb];
+  const int64_t b1 = A.bptrI[I + 1];
+  const int64_t e0 = A.bptrI[I] + (int64_t)c * kStagePostings;
+  const int64_t rem = b1 - e0;
+  const int P = rem <= 0 ? 0 : (rem < kStagePostings ? (int)rem : kStagePostings);
   TailI T;
-  T.G = (int)(gb - ga);
-  T.any = T.G > 0;
-  for (int w = ltid; w < kBuckets; w += NT) S.hash[w] = make_uint4(0u, 0u, 0u, 0u);
-  tail_sync<NT, BAR>();
-  uint32_t* slots = reinterpret_cast<uint32_t*>(S.hash);
-  for (int g = ltid; g < T.G; g += NT) {
-    const uint32_t f = A.gfeatI[ga + g];
-    S.gs[g] = (uint16_t)(A.gstartI[ga + g] - e0);
-    const uint32_t key = ((f + 1u) << 12) | (uint32_t)g;
-    uint32_t b = tail_bucket(f);
-    for (int probe = 0; probe < kBuckets; ++probe) {
-      bool done = false;
-#pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        if (atomicCAS(&slots[b * 4 + k], 0u, key) == 0u) {
-          done = true;
-          break;
-        }
-      }
-      if (done) break;
-      b = (b + 1u) & (kBuckets - 1);
-    }
+  T.P = P;
+  T.any = P > 0;
+  if (P == 0) {
+    for (int b = ltid; b <= (int)kTailBuckets; b += NT) S.boff[b] = 0;
   }
-  if (ltid == 0) S.gs[T.G] = (uint16_t)(e1 - e0);
-  for (uint32_t e = ltid; e < e1 - e0; e += NT) {
-    S.er[e] = A.bilI_r[e0 + e];
-    S.eu[e] = A.bilI_u[e0 + e];
+  for (int e = ltid; e < P; e += NT) {
+    const uint32_t key = __ldg(&A.bilI_key[e0 + e]);
+    S.et[e] = (uint16_t)(key & 0x7fffu);
+    S.eu[e] = __ldg(&A.bilI_u[e0 + e]);
+    int len = __ldg(&A.bilI_len[e0 + e]);
+    if (e == 0 && len == 0) {
+      // the chunk starts inside a run: measure what is left of it
+      const uint32_t fk = key >> 7;
+      len = 1;
+      while (len < P && len < kBlockRows && (__ldg(&A.bilI_key[e0 + len]) >> 7) == fk) ++len;
+    }
+    S.en[e] = (uint8_t)(len < P - e ? len : P - e);
+    // offsets: this posting starts every bucket after its predecessor's
+    const int bk = (int)(key >> 15);
+    const int bp = e > 0 ? (int)(__ldg(&A.bilI_key[e0 + e - 1]) >> 15) : -1;
+    for (int b = bp + 1; b <= bk; ++b) S.boff[b] = (uint16_t)e;
+    if (e == P - 1)
+      for (int b = bk + 1; b <= (int)kTailBuckets; ++b) S.boff[b] = (uint16_t)P;
   }
   tail_sync<NT, BAR>();
   return T;
 }
 
-// Group of feature f in the staged chunk, or -1.
-__device__ __forceinline__ int find_group(const TailStage& S, uint32_t f) {
-  const uint32_t want = f + 1u;
-  uint32_t b = tail_bucket(f);
-  for (int probe = 0; probe < kBuckets; ++probe) {
-    const uint4 q = S.hash[b];
-    if ((q.x >> 12) == want) return (int)(q.x & 0xfffu);
-    if ((q.y >> 12) == want) return (int)(q.y & 0xfffu);
-    if ((q.z >> 12) == want) return (int)(q.z & 0xfffu);
-    if ((q.w >> 12) == want) return (int)(q.w & 0xfffu);
-    if (q.w == 0u) return -1;  // a bucket fills in slot order: not full, not here
-    b = (b + 1u) & (kBuckets - 1);
+// Products of one J posting (feature f, column c, value v) with the staged
+// I postings of feature f.
+__device__ __forceinline__ void tail_probe(const TailStage& S, uint32_t f, int c, float v,
+                                           int* acc, int ld) {
+  const uint32_t b = f & (kTailBuckets - 1u);
+  const uint32_t tag = f >> kTailBucketBits;
+  int e = S.boff[b];
+  const int e1 = S.boff[b + 1];
+  while (e < e1) {
+    const uint32_t tg = (uint32_t)S.et[e] >> 7;
+    const int len = S.en[e];
+    if (tg < tag) {
+      e += len > 0 ? len : 1;  // next run of the bucket (every run start has len >= 1)
+      continue;
+    }
+    if (tg == tag) {
+      int* col = acc + c;
+      const int ee = e + len;
+      for (; e + 1 < ee; e += 2) {
+        const uint32_t t0 = S.et[e], t1 = S.et[e + 1];
+        const float u0 = S.eu[e], u1 = S.eu[e + 1];
+        atomicAdd(col + (int)(t0 & 127u) * ld, tail_fixed(u0 * v));
+        atomicAdd(col + (int)(t1 & 127u) * ld, tail_fixed(u1 * v));
+      }
+      if (e < ee) atomicAdd(col + (int)(S.et[e] & 127u) * ld, tail_fixed(S.eu[e] * v));
+    }
+    break;
   }
-  return -1;
-}
-
-// Products of one matched J posting (column c, value v) with group g.
-__device__ __forceinline__ void tail_products(const TailStage& S, int g, int c, float v, int* acc,
-                                              int ld) {
-  const uint32_t eb = S.gs[g], ee = S.gs[g + 1];
-  int* col = acc + c;
-  uint32_t e = eb;
-  for (; e + 1 < ee; e += 2) {
-    const int r0 = S.er[e], r1 = S.er[e + 1];
-    const float u0 = S.eu[e], u1 = S.eu[e + 1];
-    atomicAdd(col + r0 * ld, tail_fixed(u0 * v));
-    atomicAdd(col + r1 * ld, tail_fixed(u1 * v));
-  }
-  if (e < ee) atomicAdd(col + (int)S.er[e] * ld, tail_fixed(S.eu[e] * v));
 }
 
 // Tail contributions of the J postings [k0, k1) (column = record & 0xff,
@@ -164,9 +169,8 @@ __device__ __forceinline__ void tail_postings(const TileArgs& A, const TailStage
 #pragma unroll
     for (int q = 0; q < NB; ++q) {
       if (rec[q].x == 0xffffffffu) break;  // the rest of the batch is past the range
-      const int g = find_group(S, rec[q].x >> 8);
-      if (g >= 0)
-        tail_products(S, g, (int)(rec[q].x & 0xffu) - cofs, __uint_as_float(rec[q].y), acc, ld);
+      tail_probe(S, rec[q].x >> 8, (int)(rec[q].x & 0xffu) - cofs, __uint_as_float(rec[q].y),
+                 acc, ld);
     }
   }
 }

@@ -43,11 +43,8 @@ constexpr int kSliceBytes = kSlice * 4;           // 16 KB
 constexpr int kAccLd = kBlockRows + 4;            // padded accumulator row
 constexpr size_t kOffAcc = 4 * (size_t)kSliceBytes;
 constexpr size_t kOffBar = kOffAcc + (size_t)kBlockRows * kAccLd * 4;
-constexpr size_t kOffHash = kOffBar + 64;                       // 16-byte aligned
-constexpr size_t kOffEu = kOffHash + (size_t)kBuckets * 16;
-constexpr size_t kOffGs = kOffEu + (size_t)kChunkPostings * 4;
-constexpr size_t kOffEr = kOffGs + ((size_t)kChunkGroups + 8) * 2;
-constexpr size_t kSmemBytes = kOffEr + (size_t)kChunkPostings;
+constexpr size_t kOffTail = kOffBar + 64;                       // 16-byte aligned
+constexpr size_t kSmemBytes = kOffTail + kTailStageBytes;
 static_assert(kSmemBytes + 256 <= 232448, "shared memory budget");
 
 struct Smem {
@@ -66,11 +63,7 @@ __device__ __forceinline__ Smem carve(unsigned char* base) {
   s.b[1] = s.b[0] + kSlice;
   s.acc = reinterpret_cast<float*>(base + kOffAcc);
   s.bar = reinterpret_cast<uint64_t*>(base + kOffBar);
-  s.ts.hash = reinterpret_cast<uint4*>(base + kOffHash);
-  s.ts.eu = reinterpret_cast<float*>(base + kOffEu);
-  s.ts.gs = reinterpret_cast<uint16_t*>(base + kOffGs);
-  s.ts.er = reinterpret_cast<uint8_t*>(base + kOffEr);
-  s.ts.ecap = kChunkPostings;
+  s.ts = tail_stage_at(base + kOffTail);
   return s;
 }
 

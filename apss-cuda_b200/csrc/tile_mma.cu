@@ -69,9 +69,9 @@ struct SmemM {
 __host__ __device__ constexpr size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
 struct Layout {
-  size_t acc, hnj, bars, tmem, abort, hash, eu, gs, er, total;
+  size_t acc, hnj, bars, tmem, abort, tail, total;
   __host__ __device__ constexpr Layout()
-      : acc(0), hnj(0), bars(0), tmem(0), abort(0), hash(0), eu(0), gs(0), er(0), total(0) {
+      : acc(0), hnj(0), bars(0), tmem(0), abort(0), tail(0), total(0) {
     size_t o = (size_t)kStages * 2 * kTileBytes;
     acc = o;
     o += (size_t)kBlockRows * kAccLd * 4;
@@ -83,14 +83,8 @@ struct Layout {
     o = tmem + 16;
     abort = o;
     o += 16;
-    hash = align_up(o, 16);
-    o = hash + (size_t)kBuckets * 16;
-    eu = align_up(o, 16);
-    o = eu + (size_t)kChunkPostings * 4;
-    gs = align_up(o, 16);
-    o = gs + ((size_t)kChunkGroups + 8) * 2;
-    er = align_up(o, 16);
-    o = er + (size_t)kChunkPostings;
+    tail = align_up(o, 16);
+    o = tail + kTailStageBytes;
     total = align_up(o, 16);
   }
 };
@@ -112,11 +106,7 @@ __device__ __forceinline__ SmemM carve(uint8_t* raw) {
   s.drain = b + 2 * kStages + 4;
   s.tmem_base = reinterpret_cast<uint32_t*>(base + kLayout.tmem);
   s.abort = reinterpret_cast<int*>(base + kLayout.abort);
-  s.ts.hash = reinterpret_cast<uint4*>(base + kLayout.hash);
-  s.ts.eu = reinterpret_cast<float*>(base + kLayout.eu);
-  s.ts.gs = reinterpret_cast<uint16_t*>(base + kLayout.gs);
-  s.ts.er = base + kLayout.er;
-  s.ts.ecap = kChunkPostings;
+  s.ts = tail_stage_at(base + kLayout.tail);
   return s;
 }
 

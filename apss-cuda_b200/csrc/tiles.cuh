@@ -21,14 +21,10 @@ struct TileArgs {
   int nbI;
   const int32_t* blkmaxI;
   const float* hnormI;
-  const int64_t* gptrI;     // groups of each I block
-  const uint32_t* gstartI;  // entries of each group
-  const uint32_t* gfeatI;   // feature of each group
-  const int64_t* chunk_ptrI;  // staging-chunk boundaries of each I block
-  const int64_t* chunk_gI;
-  const uint32_t* bilI_f;
-  const uint8_t* bilI_r;
+  const int64_t* bptrI;     // tail postings of each I block
+  const uint32_t* bilI_key; // {bucket << 15 | tag << 7 | row}, (bucket, tag, row) order
   const float* bilI_u;
+  const uint8_t* bilI_len;  // feature run length at its first posting
   // J side (columns of the tile)
   const float* headJ32;
   const void* headJ16;
