@@ -44,17 +44,21 @@ inline unsigned grid_for(int64_t work, int threads) {
   return (unsigned)std::min<int64_t>(g, 148 * 16);
 }
 
-// tab[3q..3q+2] = {first slot, first caller row, rows} of instance q of a
-// bucket; slots [S, S + ceil(n/128)*128) hold its rows, then empty rows.
+// tab[4q..4q+3] = {first slot, first caller row, rows, threshold bits} of
+// instance q of a bucket; slots [S, S + ceil(n/128)*128) hold its rows, then
+// empty rows; every slot gets the instance's threshold.
 __global__ void k_slot_rows(const int64_t* __restrict__ tab, int k, const int64_t* __restrict__ rp,
-                            int32_t* __restrict__ slot_row, int64_t* __restrict__ len) {
+                            int32_t* __restrict__ slot_row, int64_t* __restrict__ len,
+                            float* __restrict__ t_row) {
   for (int q = blockIdx.x; q < k; q += gridDim.x) {
-    const int64_t S = tab[3 * q], R = tab[3 * q + 1], n = tab[3 * q + 2];
+    const int64_t S = tab[4 * q], R = tab[4 * q + 1], n = tab[4 * q + 2];
+    const float t = __int_as_float((int)tab[4 * q + 3]);
     const int64_t npad = (n + kBlockRows - 1) / kBlockRows * kBlockRows;
     for (int64_t r = threadIdx.x; r < npad; r += blockDim.x) {
       const bool real = r < n;
       slot_row[S + r] = real ? (int32_t)(R + r) : -1;
       len[S + r] = real ? rp[R + r + 1] - rp[R + r] : 0;
+      t_row[S + r] = t;
     }
   }
 }
@@ -96,7 +100,7 @@ struct Bucket {
   int32_t* col = nullptr;
   float* val = nullptr;
   int32_t* slot_row = nullptr;
-  float* t_blk = nullptr;
+  float* t_row = nullptr;
   int4* units = nullptr;
   int nunits = 0;
   int grid = 0;
@@ -123,18 +127,18 @@ cuapss_status prepare_bucket(cuapss_ctx* ctx, const BatchIn& in, Bucket& b, int 
   Workspace& ws = ctx->ws;
   const std::string t = tag + ":";
   const int kq = (int)b.inst.size();
-  std::vector<int64_t> tab(3 * (size_t)std::max(kq, 1));
-  std::vector<float> tblk;
+  std::vector<int64_t> tab(4 * (size_t)std::max(kq, 1));
   int64_t S = 0;
   for (int i = 0; i < kq; ++i) {
     const int q = b.inst[i];
     const int64_t n = in.inst_ptr[q + 1] - in.inst_ptr[q];
-    tab[3 * i] = S;
-    tab[3 * i + 1] = in.inst_ptr[q];
-    tab[3 * i + 2] = n;
-    const int64_t nbq = ceil_div(n, kBlockRows);
-    for (int64_t j = 0; j < nbq; ++j) tblk.push_back(in.t[q]);
-    S += nbq * kBlockRows;
+    int tbits = 0;
+    std::memcpy(&tbits, &in.t[q], sizeof(float));
+    tab[4 * i] = S;
+    tab[4 * i + 1] = in.inst_ptr[q];
+    tab[4 * i + 2] = n;
+    tab[4 * i + 3] = tbits;
+    S += ceil_div(n, kBlockRows) * kBlockRows;
   }
   b.nslots = S;
   b.nb = (int)(S / kBlockRows);
@@ -145,14 +149,11 @@ cuapss_status prepare_bucket(cuapss_ctx* ctx, const BatchIn& in, Bucket& b, int 
   ST_TRY(ws.get(t + "slot_row", (size_t)S + 1, &b.slot_row));
   ST_TRY(ws.get(t + "len", (size_t)S + 1, &len));
   ST_TRY(ws.get(t + "rp", (size_t)S + 1, &b.rp));
-  ST_TRY(ws.get(t + "tblk", std::max<size_t>(tblk.size(), 1), &b.t_blk));
+  ST_TRY(ws.get(t + "trow", (size_t)S + 1, &b.t_row));
   CU_TRY(cudaMemcpyAsync(d_tab, tab.data(), sizeof(int64_t) * tab.size(), cudaMemcpyHostToDevice,
                          st));
-  if (!tblk.empty())
-    CU_TRY(cudaMemcpyAsync(b.t_blk, tblk.data(), sizeof(float) * tblk.size(),
-                           cudaMemcpyHostToDevice, st));
   k_slot_rows<<<grid_for((int64_t)kq * kThreads, kThreads), kThreads, 0, st>>>(
-      d_tab, kq, in.x.rp, b.slot_row, len);
+      d_tab, kq, in.x.rp, b.slot_row, len, b.t_row);
   LAUNCH_CHECK();
   ST_TRY(exclusive_scan<int64_t>(len, b.rp, S, b.rp + S, ws, t + "rpscan", st));
   CU_TRY(cudaMemcpyAsync(&b.nnz, b.rp + S, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
@@ -198,7 +199,7 @@ cuapss_status prepare_bucket(cuapss_ctx* ctx, const BatchIn& in, Bucket& b, int 
   ta.p = s.p;
   ta.self = 1;
   ta.t = 1.0f;
-  ta.t_blk = b.t_blk;
+  ta.t_row = b.t_row;
   set_tile_margins(ta, in.nrm * in.nrm, in.mixed);
   // ---- units: blocks of one instance only, cost-balanced as in a single join
   std::vector<int4> units;
@@ -207,15 +208,15 @@ cuapss_status prepare_bucket(cuapss_ctx* ctx, const BatchIn& in, Bucket& b, int 
   double total = 0.0;
   b.ntiles = 0;
   for (int i = 0; i < kq; ++i) {
-    const int B0 = (int)(tab[3 * i] / kBlockRows);
-    const int B1 = B0 + (int)ceil_div(tab[3 * i + 2], kBlockRows);
+    const int B0 = (int)(tab[4 * i] / kBlockRows);
+    const int B1 = B0 + (int)ceil_div(tab[4 * i + 2], kBlockRows);
     for (int I = B0; I < B1; ++I) total += weight(I) * (B1 - I);
     b.ntiles += (int64_t)(B1 - B0) * (B1 - B0 + 1) / 2;
   }
   const double target = std::max(1.0, total / (ctx->sms * 16.0));
   for (int i = 0; i < kq; ++i) {
-    const int B0 = (int)(tab[3 * i] / kBlockRows);
-    const int B1 = B0 + (int)ceil_div(tab[3 * i + 2], kBlockRows);
+    const int B0 = (int)(tab[4 * i] / kBlockRows);
+    const int B1 = B0 + (int)ceil_div(tab[4 * i + 2], kBlockRows);
     for (int I = B0; I < B1; ++I) {
       const int chunk = (int)std::max(1.0, std::floor(target / weight(I)));
       for (int j0 = I; j0 < B1; j0 += chunk)
@@ -530,7 +531,7 @@ cuapss_status batch_device(cuapss_ctx* ctx, const DevCsr& x, int k, const int64_
     fa.colI = fa.colJ = b.col;
     fa.valI = fa.valJ = b.val;
     fa.t = 1.0f;
-    fa.t_blk = b.t_blk;
+    fa.t_row = b.t_row;
     fa.slot_row = b.slot_row;
     fa.eps_c1 = b.ta.eps_c1;
     fa.eps_c0 = b.ta.eps_c0;

@@ -117,6 +117,17 @@ class Workspace {
     for (auto& kv : bufs_) cudaFree(kv.second.ptr);
     bufs_.clear();
   }
+  // Frees the buffers whose names start with prefix.
+  void release_prefix(const std::string& prefix) {
+    for (auto it = bufs_.begin(); it != bufs_.end();) {
+      if (it->first.compare(0, prefix.size(), prefix) == 0) {
+        cudaFree(it->second.ptr);
+        it = bufs_.erase(it);
+      } else {
+        ++it;
+      }
+    }
+  }
 
  private:
   struct Buf {

@@ -79,7 +79,7 @@ __global__ void __launch_bounds__(kThreads) k_finalize(const FinalizeArgs A) {
     double eps = A.eps_c1 * K + A.eps_c0;
     if (A.eps_head > 0.0) eps += A.eps_head * (double)A.hnormI[inew] * (double)A.hnormJ[jnew];
     const double lo = (double)st - eps, hi = (double)st + eps;
-    const double t = A.t_blk ? (double)A.t_blk[inew / kBlockRows] : (double)A.t;
+    const double t = A.t_row ? (double)A.t_row[inew] : (double)A.t;
     if (hi < t) continue;
     const int32_t oi = A.rowpermI[inew], oj = A.rowpermJ[jnew];
     const int64_t ai = A.rpI[oi], an = A.rpI[oi + 1] - ai;
@@ -104,7 +104,7 @@ __global__ void __launch_bounds__(kThreads) k_finalize(const FinalizeArgs A) {
       rj = A.slot_row[oj];
       if (ri < 0 || rj < 0) continue;  // padding rows (empty) of a batched layout
     }
-    uint64_t a = (uint64_t)ri, b = (uint64_t)rj;
+    uint64_t a = (uint64_t)ri, b = (uint64_t)((int64_t)rj + A.j_offset);
     if (A.self && a > b) {
       const uint64_t tmp = a;
       a = b;

@@ -161,8 +161,15 @@ __global__ void __launch_bounds__(kThreads, 1) k_tiles_fp32(const TileArgs A) {
         const int colsJ = (int)(A.nJ - col0 < kBlockRows ? A.nJ - col0 : kBlockRows);
         const bool diag = A.self && (I == J);
         const int kmax = min(A.blkmaxI[I], A.blkmaxJ[J]);
-        const float t_lo = __double2float_rd((double)(A.t_blk ? A.t_blk[I] : A.t) -
-                                             (A.eps_c1 * kmax + A.eps_c0));
+        const double margin = A.eps_c1 * kmax + A.eps_c0;
+        float t_lo[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+          const int r = (i < 4) ? ty * 4 + i : 64 + ty * 4 + (i - 4);
+          const double tr =
+              A.t_row ? (r < rowsI ? (double)A.t_row[row0 + r] : 2.0) : (double)A.t;
+          t_lo[i] = __double2float_rd(tr - margin);
+        }
         unsigned long long pass = 0ull;
 #pragma unroll
         for (int i = 0; i < 8; ++i) {
@@ -181,7 +188,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_tiles_fp32(const TileArgs A) {
             const int c = (j < 4) ? tx * 4 + j : 64 + tx * 4 + (j - 4);
             const float s = h[i][j] + tv[j];
             h[i][j] = s;
-            const bool ok = (s >= t_lo) && (r < rowsI) && (c < colsJ) && (!diag || c > r);
+            const bool ok = (s >= t_lo[i]) && (r < rowsI) && (c < colsJ) && (!diag || c > r);
             pass |= (unsigned long long)ok << (i * 8 + j);
           }
         }

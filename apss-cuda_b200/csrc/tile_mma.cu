@@ -256,14 +256,14 @@ __global__ void __launch_bounds__(kThreads, 1) k_tiles_mma(const TileArgs A, con
       TailI T{};
       if (nch == 1) T = stage_tail_chunk<kCT, kComputeBar>(A, S.ts, I, 0, ctid);
       const float hn_r = row < rowsI ? A.hnormI[row0 + row] : 0.0f;
+      const double t_r = A.t_row ? (row < rowsI ? (double)A.t_row[row0 + row] : 2.0) : (double)A.t;
       for (int J = U.y; ok && J < U.z; ++J, ++tt) {
         const uint32_t b = tt & 1u, tround = tt >> 1;
         const int64_t col0 = (int64_t)J * kBlockRows;
         const int colsJ = (int)(A.nJ - col0 < kBlockRows ? A.nJ - col0 : kBlockRows);
         const bool diag = A.self && (I == J);
         const int kmax = min(A.blkmaxI[I], A.blkmaxJ[J]);
-        const float t_lo = __double2float_rd((double)(A.t_blk ? A.t_blk[I] : A.t) -
-                                             (A.eps_c1 * kmax + A.eps_c0));
+        const float t_lo = __double2float_rd(t_r - (A.eps_c1 * kmax + A.eps_c0));
         if (ctid < kBlockRows)
           S.hnj[ctid] =
               ctid < colsJ ? __double2float_ru(A.eps_head * (double)A.hnormJ[col0 + ctid]) : 0.0f;

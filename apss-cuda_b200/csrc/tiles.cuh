@@ -37,7 +37,7 @@ struct TileArgs {
   int p;
   int self;
   float t;
-  const float* t_blk;  // per I block threshold (batched instances), or null: t
+  const float* t_row;  // threshold of each I row (batched instances, queries), or null: t
   double eps_c1;  // FP32 error margin of a tile: eps_c1 * min(maxnnz_I, maxnnz_J) + eps_c0
   double eps_c0;
   double eps_head;  // tensor-core path: extra margin per unit of ||a_h|| ||b_h||
@@ -103,8 +103,9 @@ struct FinalizeArgs {
   const int32_t* colJ;
   const float* valJ;
   float t;
-  const float* t_blk;       // per I row block threshold, or null: t
+  const float* t_row;       // threshold of each I row, or null: t
   const int32_t* slot_row;  // side row -> caller's row (-1: padding), or null: rowperm
+  int64_t j_offset;         // added to the J row of every output pair (index segments)
   double eps_c1;
   double eps_c0;
   double eps_head;

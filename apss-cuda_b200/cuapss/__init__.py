@@ -99,7 +99,8 @@ _lib = None
 EXPORTED = [
     "cuapss_default_opts", "cuapss_status_string", "cuapss_abi_version", "cuapss_create",
     "cuapss_destroy", "cuapss_run", "cuapss_join", "cuapss_build_index", "cuapss_feature_remap",
-    "cuapss_batch_run",
+    "cuapss_batch_run", "cuapss_index_create", "cuapss_index_append", "cuapss_index_query",
+    "cuapss_index_info", "cuapss_index_destroy",
 ]
 
 
@@ -134,6 +135,20 @@ def lib():
         L.cuapss_batch_run.argtypes = [_P, ctypes.POINTER(CsrDesc), ctypes.c_int32, _P, _P,
                                        ctypes.POINTER(PairsDesc), ctypes.POINTER(Stats), _P]
         L.cuapss_batch_run.restype = ctypes.c_int
+        L.cuapss_index_create.argtypes = [_P, ctypes.POINTER(CsrDesc), ctypes.POINTER(_P)]
+        L.cuapss_index_create.restype = ctypes.c_int
+        L.cuapss_index_append.argtypes = [_P, _P, ctypes.POINTER(CsrDesc)]
+        L.cuapss_index_append.restype = ctypes.c_int
+        L.cuapss_index_query.argtypes = [_P, _P, ctypes.POINTER(CsrDesc), _P,
+                                         ctypes.POINTER(PairsDesc), ctypes.POINTER(Stats)]
+        L.cuapss_index_query.restype = ctypes.c_int
+        L.cuapss_index_info.argtypes = [_P, ctypes.POINTER(ctypes.c_int64),
+                                        ctypes.POINTER(ctypes.c_int32),
+                                        ctypes.POINTER(ctypes.c_int32),
+                                        ctypes.POINTER(ctypes.c_int64)]
+        L.cuapss_index_info.restype = ctypes.c_int
+        L.cuapss_index_destroy.argtypes = [_P]
+        L.cuapss_index_destroy.restype = ctypes.c_int
         _lib = L
     return _lib
 
@@ -316,3 +331,67 @@ class Context:
         _check(lib().cuapss_feature_remap(self._h, ctypes.byref(d), perm.ctypes.data,
                                           counts.ctypes.data), "cuapss_feature_remap")
         return perm, counts
+
+
+class Index:
+    """Resident index (cuapss_index_*): rows kept in HBM for repeated query
+    batches with per-query thresholds; appends add rows."""
+
+    def __init__(self, ctx: "Context", x):
+        self.ctx = ctx
+        self._h = _P()
+        d, keep = _desc(x)
+        _check(lib().cuapss_index_create(ctx._h, ctypes.byref(d), ctypes.byref(self._h)),
+               "cuapss_index_create")
+
+    def append(self, x, ctx: "Context | None" = None):
+        d, keep = _desc(x)
+        c = ctx or self.ctx
+        _check(lib().cuapss_index_append(c._h, self._h, ctypes.byref(d)), "cuapss_index_append")
+
+    def info(self) -> dict:
+        r, s, p, b = ctypes.c_int64(), ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int64()
+        _check(lib().cuapss_index_info(self._h, ctypes.byref(r), ctypes.byref(s), ctypes.byref(p),
+                                       ctypes.byref(b)), "cuapss_index_info")
+        return {"rows": r.value, "segments": s.value, "head_width": p.value,
+                "device_bytes": b.value}
+
+    def query(self, q, t, capacity: int = 1 << 16, ctx: "Context | None" = None):
+        """(i = query row, j = index row, sim), sorted by (i, j); t is one
+        threshold or one per query row."""
+        c = ctx or self.ctx
+        d, keep = _desc(q)
+        tq = np.ascontiguousarray(np.broadcast_to(np.asarray(t, np.float32), (d.n,)))
+        cap = max(int(capacity), 1)
+        while True:
+            oi = np.empty(cap, np.int32)
+            oj = np.empty(cap, np.int32)
+            os_ = np.empty(cap, np.float32)
+            pr = PairsDesc(oi.ctypes.data, oj.ctypes.data, os_.ctypes.data, cap, 0, 0)
+            st = Stats()
+            s = lib().cuapss_index_query(c._h, self._h, ctypes.byref(d), tq.ctypes.data,
+                                         ctypes.byref(pr), ctypes.byref(st))
+            if s == EOVERFLOW:
+                cap = int(pr.count)
+                continue
+            _check(s, "cuapss_index_query")
+            c.last_stats = st.as_dict()
+            n = int(pr.count)
+            return oi[:n].copy(), oj[:n].copy(), os_[:n].copy()
+
+    def close(self):
+        if self._h:
+            lib().cuapss_index_destroy(self._h)
+            self._h = _P()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -143,6 +143,49 @@ cuapss_status cuapss_join(cuapss_ctx* ctx, const cuapss_csr* a,
                           const cuapss_csr* b, float t, cuapss_pairs* out,
                           cuapss_stats* stats);
 
+/* ---- Resident index for serving ------------------------------------------
+ * An index keeps a matrix resident in HBM, prepared for repeated query
+ * batches: the frequency remap (fixed at creation), the dense head block and
+ * the tail inverted lists of its rows, and a copy of its CSR for the exact
+ * finalize. Appends add rows as a new immutable segment (its lists are built
+ * for the new rows only); segments of similar size are merged, so an index of
+ * N rows has O(log N) segments. A query batch (q rows, each with its own
+ * threshold t[i]) returns every (query row i, index row j) with
+ * sim >= t[i], sorted by (i, j), under the exactness contract above.
+ *
+ * Concurrency: one index may be queried from several contexts (host threads,
+ * streams) at once and appended to from one of them; a query sees the
+ * segments that existed when it started. The index's device and precision
+ * are those of the context that created it; contexts used with it must be on
+ * the same device.
+ *
+ * The reference has no resident index: similarity_join_device rebuilds every
+ * partition's index on each call (similarity_search.cu:1075-1272). */
+typedef struct cuapss_index cuapss_index;
+
+/* Build an index over the rows of x (host or device CSR; copied). */
+cuapss_status cuapss_index_create(cuapss_ctx* ctx, const cuapss_csr* x,
+                                  cuapss_index** idx);
+
+/* Append the rows of x (same d) as index rows [rows, rows + x->n). */
+cuapss_status cuapss_index_append(cuapss_ctx* ctx, cuapss_index* idx,
+                                  const cuapss_csr* x);
+
+/* Query batch: q rows against the index, t[i] (host array of q->n floats,
+ * each > 0) the threshold of query row i. out->i = query row, out->j = index
+ * row. Synchronous on ctx's stream. */
+cuapss_status cuapss_index_query(cuapss_ctx* ctx, const cuapss_index* idx,
+                                 const cuapss_csr* q, const float* t,
+                                 cuapss_pairs* out, cuapss_stats* stats);
+
+/* Rows, segments, head width and device bytes held by the index (any
+ * pointer may be NULL). */
+cuapss_status cuapss_index_info(const cuapss_index* idx, int64_t* rows,
+                                int32_t* segments, int32_t* head_width,
+                                int64_t* device_bytes);
+
+cuapss_status cuapss_index_destroy(cuapss_index* idx);
+
 /* Size buckets of the batched self-join (instance rows n):
  * bucket 0: n <= 1024, bucket 1: n <= 8192, bucket 2: larger. */
 #define CUAPSS_BATCH_BUCKETS 3
