@@ -31,6 +31,7 @@
 
 #include "ctx.cuh"
 #include "prep.cuh"
+#include "serve.h"
 #include "prims.cuh"
 #include "tiles.cuh"
 
@@ -347,6 +348,12 @@ extern "C" cuapss_status cuapss_index_destroy(cuapss_index* idx) {
 extern "C" cuapss_status cuapss_index_query(cuapss_ctx* ctx, const cuapss_index* idx,
                                             const cuapss_csr* qx, const float* t,
                                             cuapss_pairs* out, cuapss_stats* stats) {
+  return cuapss::index_query_rows(ctx, idx, qx, t, out, stats, nullptr);
+}
+
+cuapss_status cuapss::index_query_rows(cuapss_ctx* ctx, const cuapss_index* idx,
+                                       const cuapss_csr* qx, const float* t, cuapss_pairs* out,
+                                       cuapss_stats* stats, int64_t* rows_seen) {
   if (!ctx || !idx || !qx || !out) return CUAPSS_EINVAL;
   if (ctx->device != idx->device || qx->d != idx->d) return CUAPSS_EINVAL;
   if (out->capacity < 0 || (out->capacity > 0 && (!out->i || !out->j || !out->sim)))
@@ -369,6 +376,7 @@ extern "C" cuapss_status cuapss_index_query(cuapss_ctx* ctx, const cuapss_index*
     rows = idx->rows;
     nrm_idx = idx->nrm;
   }
+  if (rows_seen) *rows_seen = rows;
   DevCsr q;
   ST_TRY(stage_csr(ctx, qx, "QX", &q));
   double nrm_q = 1.0;

@@ -1,0 +1,391 @@
+// Request server over a resident index (cuapss_server_*): continuous
+// batching of query requests with per-query thresholds, ordered appends,
+// admission by the working memory of the batches in flight.
+//
+// Lanes. Each lane is a host thread with its own context (own CUDA stream,
+// own grow-only working memory). A free lane takes, under the queue lock, the
+// longest prefix of queued query requests (in arrival order, stopping at the
+// first queued append) that fits max_batch_rows and the memory budget,
+// concatenates their rows into one batch CSR with one threshold per row, runs
+// it with index_query_rows and hands each request its slice of the sorted
+// output (rows of one request are contiguous in the batch). Lanes run
+// concurrently, so their batches overlap on the GPU; requests that arrive
+// while batches run are picked up by the next lane that frees up.
+//
+// Admission. The working memory of a batch is estimated from its rows,
+// non-zeros and the head width, plus its expected candidates (a running
+// mean of candidates per query row, 24 bytes each for keys, values and
+// output). A batch is admitted while the estimates of all batches in flight
+// stay within hbm_budget; a lone batch is always admitted.
+//
+// Appends are taken in submission order by one lane at a time; queries queued
+// behind an append wait until some lane has taken it.
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <memory>
+#include <mutex>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "cuapss.h"
+#include "serve.h"
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+struct Request {
+  uint64_t id = 0;
+  bool append = false;
+  int64_t n = 0, d = 0;
+  std::vector<int64_t> rp;
+  std::vector<int32_t> col;
+  std::vector<float> val;
+  std::vector<float> t;
+  Clock::time_point submit, start, done;
+  bool finished = false;
+  cuapss_status status = CUAPSS_OK;
+  std::vector<int32_t> oi, oj;
+  std::vector<float> os;
+  int64_t batch_id = -1, batch_rows = 0, index_rows = 0;
+};
+
+using ReqPtr = std::shared_ptr<Request>;
+
+double ms_between(Clock::time_point a, Clock::time_point b) {
+  return std::chrono::duration<double, std::milli>(b - a).count();
+}
+
+}  // namespace
+
+struct cuapss_server {
+  cuapss_index* idx = nullptr;
+  int device = 0;
+  cuapss_server_opts opts{};
+  int head_width = 0;
+  std::vector<cuapss_ctx*> lanes;
+  std::vector<std::thread> threads;
+  std::mutex mu;
+  std::condition_variable cv_work, cv_done;
+  std::deque<ReqPtr> queue;
+  std::unordered_map<uint64_t, ReqPtr> reqs;
+  uint64_t next_id = 1;
+  int64_t next_batch = 0;
+  bool stop = false;
+  int64_t inflight_bytes = 0;
+  double cand_per_row = 64.0;  // running mean of candidates per query row
+};
+
+namespace {
+
+int64_t estimate_bytes(const cuapss_server* s, int64_t rows, int64_t nnz) {
+  const double cand = s->cand_per_row * (double)rows;
+  return (int64_t)((double)rows * (2.0 * s->head_width + 256.0) + (double)nnz * 64.0 +
+                   cand * 24.0) + (1 << 20);
+}
+
+void run_append(cuapss_server* s, cuapss_ctx* ctx, const ReqPtr& r) {
+  cuapss_csr x{r->n, r->d, (int64_t)r->col.size(), r->rp.data(), r->col.data(), r->val.data(), 0};
+  const cuapss_status st = cuapss_index_append(ctx, s->idx, &x);
+  int64_t rows = 0;
+  cuapss_index_info(s->idx, &rows, nullptr, nullptr, nullptr);
+  std::lock_guard<std::mutex> lk(s->mu);
+  r->status = st;
+  r->index_rows = rows;
+  r->done = Clock::now();
+  r->finished = true;
+  // the data is no longer needed
+  r->rp.clear();
+  r->col.clear();
+  r->val.clear();
+}
+
+void run_batch(cuapss_server* s, cuapss_ctx* ctx, std::vector<ReqPtr>& batch, int64_t batch_id,
+               int64_t est) {
+  // concatenate the requests' rows
+  int64_t rows = 0, nnz = 0;
+  for (auto& r : batch) {
+    rows += r->n;
+    nnz += (int64_t)r->col.size();
+  }
+  std::vector<int64_t> rp((size_t)rows + 1, 0);
+  std::vector<int32_t> col((size_t)std::max<int64_t>(nnz, 1));
+  std::vector<float> val((size_t)std::max<int64_t>(nnz, 1));
+  std::vector<float> t((size_t)std::max<int64_t>(rows, 1));
+  std::vector<int64_t> first((size_t)batch.size() + 1, 0);
+  {
+    int64_t ro = 0, eo = 0;
+    for (size_t k = 0; k < batch.size(); ++k) {
+      const Request& r = *batch[k];
+      first[k] = ro;
+      for (int64_t i = 0; i < r.n; ++i) rp[ro + i + 1] = eo + r.rp[i + 1];
+      std::copy(r.col.begin(), r.col.end(), col.begin() + eo);
+      std::copy(r.val.begin(), r.val.end(), val.begin() + eo);
+      std::copy(r.t.begin(), r.t.end(), t.begin() + ro);
+      ro += r.n;
+      eo += (int64_t)r.col.size();
+    }
+    first[batch.size()] = ro;
+  }
+  cuapss_csr q{rows, batch[0]->d, nnz, rp.data(), col.data(), val.data(), 0};
+  int64_t cap = std::max<int64_t>(1 << 16, rows * 16);
+  std::vector<int32_t> oi, oj;
+  std::vector<float> os;
+  cuapss_status st = CUAPSS_OK;
+  cuapss_stats stats{};
+  int64_t rows_seen = 0;
+  for (int attempt = 0; attempt < 3; ++attempt) {
+    oi.resize((size_t)cap);
+    oj.resize((size_t)cap);
+    os.resize((size_t)cap);
+    cuapss_pairs out{oi.data(), oj.data(), os.data(), cap, 0, 0};
+    st = cuapss::index_query_rows(ctx, s->idx, &q, t.data(), &out, &stats, &rows_seen);
+    if (st == CUAPSS_EOVERFLOW) {
+      cap = out.count;
+      continue;
+    }
+    if (st == CUAPSS_OK) {
+      oi.resize((size_t)out.count);
+      oj.resize((size_t)out.count);
+      os.resize((size_t)out.count);
+    }
+    break;
+  }
+  // split by request: pairs are sorted by batch row
+  std::vector<size_t> cut(batch.size() + 1, oi.size());
+  if (st == CUAPSS_OK) {
+    for (size_t k = 0; k <= batch.size(); ++k)
+      cut[k] = (size_t)(std::lower_bound(oi.begin(), oi.end(), (int32_t)first[k]) - oi.begin());
+  }
+  const Clock::time_point now = Clock::now();
+  std::lock_guard<std::mutex> lk(s->mu);
+  for (size_t k = 0; k < batch.size(); ++k) {
+    Request& r = *batch[k];
+    r.status = st;
+    if (st == CUAPSS_OK) {
+      const size_t a = cut[k], b = cut[k + 1];
+      r.oi.resize(b - a);
+      r.oj.assign(oj.begin() + a, oj.begin() + b);
+      r.os.assign(os.begin() + a, os.begin() + b);
+      for (size_t m = a; m < b; ++m) r.oi[m - a] = oi[m] - (int32_t)first[k];
+    }
+    r.batch_id = batch_id;
+    r.batch_rows = rows;
+    r.index_rows = rows_seen;
+    r.done = now;
+    r.finished = true;
+    r.rp.clear();
+    r.col.clear();
+    r.val.clear();
+  }
+  if (st == CUAPSS_OK && rows > 0) {
+    const double per = (double)stats.candidates / (double)rows;
+    s->cand_per_row = 0.8 * s->cand_per_row + 0.2 * per;
+  }
+  s->inflight_bytes -= est;
+}
+
+void lane_loop(cuapss_server* s, int lane) {
+  cuapss_ctx* ctx = s->lanes[lane];
+  for (;;) {
+    std::vector<ReqPtr> batch;
+    ReqPtr app;
+    int64_t est = 0, bid = 0;
+    {
+      std::unique_lock<std::mutex> lk(s->mu);
+      for (;;) {
+        if (!s->queue.empty()) {
+          if (s->queue.front()->append) {
+            app = s->queue.front();
+            s->queue.pop_front();
+            app->start = Clock::now();
+            break;
+          }
+          // longest admissible prefix of query requests
+          int64_t rows = 0, nnz = 0;
+          size_t k = 0;
+          for (; k < s->queue.size(); ++k) {
+            const Request& r = *s->queue[k];
+            if (r.append) break;
+            const int64_t nr = rows + r.n, nz = nnz + (int64_t)r.col.size();
+            if (k > 0 && nr > s->opts.max_batch_rows) break;
+            const int64_t e = estimate_bytes(s, nr, nz);
+            if (s->inflight_bytes + e > s->opts.hbm_budget && (k > 0 || s->inflight_bytes > 0))
+              break;
+            rows = nr;
+            nnz = nz;
+            est = e;
+          }
+          if (k > 0) {
+            const Clock::time_point now = Clock::now();
+            for (size_t m = 0; m < k; ++m) {
+              batch.push_back(s->queue.front());
+              s->queue.pop_front();
+              batch.back()->start = now;
+            }
+            s->inflight_bytes += est;
+            bid = s->next_batch++;
+            break;
+          }
+        } else if (s->stop) {
+          return;
+        }
+        s->cv_work.wait(lk);
+      }
+    }
+    if (app) run_append(s, ctx, app);
+    else run_batch(s, ctx, batch, bid, est);
+    s->cv_done.notify_all();
+    s->cv_work.notify_all();
+  }
+}
+
+cuapss_status copy_request(const cuapss_csr* x, Request* r) {
+  if (!x || x->on_device || x->n < 0 || x->nnz < 0 || !x->rowptr) return CUAPSS_EINVAL;
+  if (x->nnz > 0 && (!x->col || !x->val)) return CUAPSS_EINVAL;
+  if (x->rowptr[0] != 0 || x->rowptr[x->n] != x->nnz) return CUAPSS_EINVAL;
+  r->n = x->n;
+  r->d = x->d;
+  r->rp.assign(x->rowptr, x->rowptr + x->n + 1);
+  r->col.assign(x->col, x->col + x->nnz);
+  r->val.assign(x->val, x->val + x->nnz);
+  return CUAPSS_OK;
+}
+
+uint64_t enqueue(cuapss_server* s, ReqPtr r) {
+  std::lock_guard<std::mutex> lk(s->mu);
+  r->id = s->next_id++;
+  r->submit = Clock::now();
+  s->reqs[r->id] = r;
+  s->queue.push_back(r);
+  s->cv_work.notify_all();
+  return r->id;
+}
+
+}  // namespace
+
+extern "C" {
+
+void cuapss_server_default_opts(cuapss_server_opts* o) {
+  if (!o) return;
+  o->lanes = 3;
+  o->max_batch_rows = 4096;
+  o->hbm_budget = (int64_t)16 << 30;
+}
+
+cuapss_status cuapss_server_create(cuapss_server** out, cuapss_index* idx, int device,
+                                   const cuapss_server_opts* o) {
+  if (!out || !idx) return CUAPSS_EINVAL;
+  *out = nullptr;
+  cuapss_server_opts opts;
+  cuapss_server_default_opts(&opts);
+  if (o) opts = *o;
+  if (opts.lanes < 1 || opts.lanes > 16 || opts.max_batch_rows < 1 || opts.hbm_budget < 1)
+    return CUAPSS_EINVAL;
+  auto s = std::make_unique<cuapss_server>();
+  s->idx = idx;
+  s->device = device;
+  s->opts = opts;
+  int32_t p = 0;
+  cuapss_status st = cuapss_index_info(idx, nullptr, nullptr, &p, nullptr);
+  if (st != CUAPSS_OK) return st;
+  s->head_width = p;
+  for (int l = 0; l < opts.lanes; ++l) {
+    cuapss_opts co;
+    cuapss_default_opts(&co);
+    co.device = device;
+    cuapss_ctx* c = nullptr;
+    st = cuapss_create(&c, &co);
+    if (st != CUAPSS_OK) {
+      for (auto* x : s->lanes) cuapss_destroy(x);
+      return st;
+    }
+    s->lanes.push_back(c);
+  }
+  for (int l = 0; l < opts.lanes; ++l) s->threads.emplace_back(lane_loop, s.get(), l);
+  *out = s.release();
+  return CUAPSS_OK;
+}
+
+cuapss_status cuapss_server_submit_query(cuapss_server* s, const cuapss_csr* q, const float* t,
+                                         uint64_t* ticket) {
+  if (!s || !ticket) return CUAPSS_EINVAL;
+  auto r = std::make_shared<Request>();
+  const cuapss_status st = copy_request(q, r.get());
+  if (st != CUAPSS_OK) return st;
+  if (q->n > 0 && !t) return CUAPSS_EINVAL;
+  for (int64_t i = 0; i < q->n; ++i)
+    if (!(t[i] > 0.0f) || !(t[i] < 1e30f)) return CUAPSS_EINVAL;
+  r->t.assign(t, t + q->n);
+  *ticket = enqueue(s, r);
+  return CUAPSS_OK;
+}
+
+cuapss_status cuapss_server_submit_append(cuapss_server* s, const cuapss_csr* x,
+                                          uint64_t* ticket) {
+  if (!s || !ticket) return CUAPSS_EINVAL;
+  auto r = std::make_shared<Request>();
+  r->append = true;
+  const cuapss_status st = copy_request(x, r.get());
+  if (st != CUAPSS_OK) return st;
+  *ticket = enqueue(s, r);
+  return CUAPSS_OK;
+}
+
+cuapss_status cuapss_server_wait(cuapss_server* s, uint64_t ticket, int32_t timeout_ms,
+                                 cuapss_pairs* out, cuapss_request_info* info) {
+  if (!s) return CUAPSS_EINVAL;
+  std::unique_lock<std::mutex> lk(s->mu);
+  auto it = s->reqs.find(ticket);
+  if (it == s->reqs.end()) return CUAPSS_EINVAL;
+  ReqPtr r = it->second;
+  auto ready = [&] { return r->finished; };
+  if (timeout_ms < 0) {
+    s->cv_done.wait(lk, ready);
+  } else if (!s->cv_done.wait_for(lk, std::chrono::milliseconds(timeout_ms), ready)) {
+    return CUAPSS_ETIMEOUT;
+  }
+  if (info) {
+    info->status = r->status;
+    info->pairs = (int64_t)r->oi.size();
+    info->queue_ms = ms_between(r->submit, r->start);
+    info->latency_ms = ms_between(r->submit, r->done);
+    info->batch_id = r->batch_id;
+    info->batch_rows = r->batch_rows;
+    info->index_rows = r->index_rows;
+  }
+  if (r->status != CUAPSS_OK) {
+    s->reqs.erase(it);
+    return r->status;
+  }
+  if (out) {
+    const int64_t m = (int64_t)r->oi.size();
+    out->count = m;
+    if (m > out->capacity) return CUAPSS_EOVERFLOW;
+    if (m > 0 && (!out->i || !out->j || !out->sim || out->on_device)) return CUAPSS_EINVAL;
+    std::memcpy(out->i, r->oi.data(), sizeof(int32_t) * m);
+    std::memcpy(out->j, r->oj.data(), sizeof(int32_t) * m);
+    std::memcpy(out->sim, r->os.data(), sizeof(float) * m);
+  }
+  s->reqs.erase(it);
+  return CUAPSS_OK;
+}
+
+cuapss_status cuapss_server_destroy(cuapss_server* s) {
+  if (!s) return CUAPSS_OK;
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->stop = true;
+  }
+  s->cv_work.notify_all();
+  for (auto& th : s->threads) th.join();
+  for (auto* c : s->lanes) cuapss_destroy(c);
+  delete s;
+  return CUAPSS_OK;
+}
+
+}  // extern "C"

@@ -96,11 +96,28 @@ _P = ctypes.c_void_p
 _lib = None
 
 # Every symbol declared by include/cuapss.h (checked by the CPU tests).
+class ServerOpts(ctypes.Structure):
+    _fields_ = [("lanes", ctypes.c_int32), ("max_batch_rows", ctypes.c_int64),
+                ("hbm_budget", ctypes.c_int64)]
+
+
+class RequestInfo(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_int), ("pairs", ctypes.c_int64),
+                ("queue_ms", ctypes.c_double), ("latency_ms", ctypes.c_double),
+                ("batch_id", ctypes.c_int64), ("batch_rows", ctypes.c_int64),
+                ("index_rows", ctypes.c_int64)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 EXPORTED = [
     "cuapss_default_opts", "cuapss_status_string", "cuapss_abi_version", "cuapss_create",
     "cuapss_destroy", "cuapss_run", "cuapss_join", "cuapss_build_index", "cuapss_feature_remap",
     "cuapss_batch_run", "cuapss_index_create", "cuapss_index_append", "cuapss_index_query",
-    "cuapss_index_info", "cuapss_index_destroy",
+    "cuapss_index_info", "cuapss_index_destroy", "cuapss_server_default_opts",
+    "cuapss_server_create", "cuapss_server_submit_query", "cuapss_server_submit_append",
+    "cuapss_server_wait", "cuapss_server_destroy",
 ]
 
 
@@ -149,6 +166,22 @@ def lib():
         L.cuapss_index_info.restype = ctypes.c_int
         L.cuapss_index_destroy.argtypes = [_P]
         L.cuapss_index_destroy.restype = ctypes.c_int
+        L.cuapss_server_default_opts.argtypes = [ctypes.POINTER(ServerOpts)]
+        L.cuapss_server_default_opts.restype = None
+        L.cuapss_server_create.argtypes = [ctypes.POINTER(_P), _P, ctypes.c_int,
+                                           ctypes.POINTER(ServerOpts)]
+        L.cuapss_server_create.restype = ctypes.c_int
+        L.cuapss_server_submit_query.argtypes = [_P, ctypes.POINTER(CsrDesc), _P,
+                                                 ctypes.POINTER(ctypes.c_uint64)]
+        L.cuapss_server_submit_query.restype = ctypes.c_int
+        L.cuapss_server_submit_append.argtypes = [_P, ctypes.POINTER(CsrDesc),
+                                                  ctypes.POINTER(ctypes.c_uint64)]
+        L.cuapss_server_submit_append.restype = ctypes.c_int
+        L.cuapss_server_wait.argtypes = [_P, ctypes.c_uint64, ctypes.c_int32,
+                                         ctypes.POINTER(PairsDesc), ctypes.POINTER(RequestInfo)]
+        L.cuapss_server_wait.restype = ctypes.c_int
+        L.cuapss_server_destroy.argtypes = [_P]
+        L.cuapss_server_destroy.restype = ctypes.c_int
         _lib = L
     return _lib
 
@@ -382,6 +415,71 @@ class Index:
     def close(self):
         if self._h:
             lib().cuapss_index_destroy(self._h)
+            self._h = _P()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Server:
+    """Request server over an Index (cuapss_server_*): continuous batching
+    of query requests on several lanes, ordered appends."""
+
+    def __init__(self, index: "Index", device: int = 0, lanes: int = 3,
+                 max_batch_rows: int = 4096, hbm_budget: int = 16 << 30):
+        o = ServerOpts()
+        lib().cuapss_server_default_opts(ctypes.byref(o))
+        o.lanes, o.max_batch_rows, o.hbm_budget = lanes, max_batch_rows, hbm_budget
+        self.index = index
+        self._h = _P()
+        _check(lib().cuapss_server_create(ctypes.byref(self._h), index._h, device,
+                                          ctypes.byref(o)), "cuapss_server_create")
+
+    def submit_query(self, q: Csr, t) -> int:
+        d, keep = _desc(q)
+        tq = np.ascontiguousarray(np.broadcast_to(np.asarray(t, np.float32), (d.n,)))
+        tk = ctypes.c_uint64()
+        _check(lib().cuapss_server_submit_query(self._h, ctypes.byref(d), tq.ctypes.data,
+                                                ctypes.byref(tk)), "cuapss_server_submit_query")
+        return tk.value
+
+    def submit_append(self, x: Csr) -> int:
+        d, keep = _desc(x)
+        tk = ctypes.c_uint64()
+        _check(lib().cuapss_server_submit_append(self._h, ctypes.byref(d), ctypes.byref(tk)),
+               "cuapss_server_submit_append")
+        return tk.value
+
+    def wait(self, ticket: int, timeout_ms: int = -1, capacity: int = 1 << 16):
+        """((i, j, sim), info) of a request; i numbered within the request."""
+        cap = max(int(capacity), 1)
+        while True:
+            oi = np.empty(cap, np.int32)
+            oj = np.empty(cap, np.int32)
+            os_ = np.empty(cap, np.float32)
+            pr = PairsDesc(oi.ctypes.data, oj.ctypes.data, os_.ctypes.data, cap, 0, 0)
+            info = RequestInfo()
+            s = lib().cuapss_server_wait(self._h, int(ticket), int(timeout_ms), ctypes.byref(pr),
+                                         ctypes.byref(info))
+            if s == EOVERFLOW:
+                cap = int(pr.count)
+                continue
+            _check(s, "cuapss_server_wait")
+            n = int(pr.count)
+            return (oi[:n].copy(), oj[:n].copy(), os_[:n].copy()), info.as_dict()
+
+    def close(self):
+        if self._h:
+            lib().cuapss_server_destroy(self._h)
             self._h = _P()
 
     def __enter__(self):

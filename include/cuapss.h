@@ -186,6 +186,61 @@ cuapss_status cuapss_index_info(const cuapss_index* idx, int64_t* rows,
 
 cuapss_status cuapss_index_destroy(cuapss_index* idx);
 
+/* ---- Request server over a resident index (continuous batching) ----------
+ * Requests (query batches with per-query thresholds, or appends) are queued
+ * as they arrive. Each of `lanes` host threads owns a context (its own
+ * stream and working memory); whenever a lane is free it merges the queued
+ * query requests, in arrival order, into one batch (at most max_batch_rows
+ * query rows, and admitted only while the estimated working memory of all
+ * batches in flight stays within hbm_budget) and runs it, so requests that
+ * arrive while others are on the GPU join the next batch and batches of
+ * different lanes overlap on the device. Appends are applied in submission
+ * order, one at a time; a query sees the rows appended before its batch
+ * started (cuapss_request_info.index_rows). No counterpart in the reference,
+ * which has no request path. */
+typedef struct cuapss_server cuapss_server;
+
+typedef struct {
+  int32_t lanes;           /* batches in flight, default 3 */
+  int64_t max_batch_rows;  /* query rows per batch, default 4096 */
+  int64_t hbm_budget;      /* working-memory bytes of batches in flight,
+                              default 16 GiB */
+} cuapss_server_opts;
+
+typedef struct {
+  cuapss_status status;  /* the request's own outcome */
+  int64_t pairs;         /* pairs of this request */
+  double queue_ms;       /* submit -> its batch started */
+  double latency_ms;     /* submit -> results ready */
+  int64_t batch_id;      /* batch it ran in (query requests) */
+  int64_t batch_rows;    /* query rows of that batch */
+  int64_t index_rows;    /* index rows it was matched against / after append */
+} cuapss_request_info;
+
+void cuapss_server_default_opts(cuapss_server_opts* o);
+
+/* The server uses idx (which must outlive it) on `device`. */
+cuapss_status cuapss_server_create(cuapss_server** s, cuapss_index* idx, int device,
+                                   const cuapss_server_opts* o);
+
+/* Queue a query request: q (host CSR, copied) with thresholds t[q->n]. */
+cuapss_status cuapss_server_submit_query(cuapss_server* s, const cuapss_csr* q,
+                                         const float* t, uint64_t* ticket);
+
+/* Queue an append of the rows of x (host CSR, copied). */
+cuapss_status cuapss_server_submit_append(cuapss_server* s, const cuapss_csr* x,
+                                          uint64_t* ticket);
+
+/* Wait up to timeout_ms (< 0: no limit) for a request. On success its pairs
+ * (query rows numbered within the request) are copied to out (host arrays)
+ * and the request is released; CUAPSS_EOVERFLOW sets out->count to the
+ * required capacity and keeps the request; CUAPSS_ETIMEOUT if not done. */
+cuapss_status cuapss_server_wait(cuapss_server* s, uint64_t ticket, int32_t timeout_ms,
+                                 cuapss_pairs* out, cuapss_request_info* info);
+
+/* Finishes the queued requests, stops the lanes, frees the server. */
+cuapss_status cuapss_server_destroy(cuapss_server* s);
+
 /* Size buckets of the batched self-join (instance rows n):
  * bucket 0: n <= 1024, bucket 1: n <= 8192, bucket 2: larger. */
 #define CUAPSS_BATCH_BUCKETS 3
