@@ -273,7 +273,7 @@ extern "C" {
 void cuapss_server_default_opts(cuapss_server_opts* o) {
   if (!o) return;
   o->lanes = 3;
-  o->max_batch_rows = 4096;
+  o->max_batch_rows = 1024;
   o->hbm_budget = (int64_t)16 << 30;
 }
 

@@ -435,7 +435,7 @@ class Server:
     of query requests on several lanes, ordered appends."""
 
     def __init__(self, index: "Index", device: int = 0, lanes: int = 3,
-                 max_batch_rows: int = 4096, hbm_budget: int = 16 << 30):
+                 max_batch_rows: int = 1024, hbm_budget: int = 16 << 30):
         o = ServerOpts()
         lib().cuapss_server_default_opts(ctypes.byref(o))
         o.lanes, o.max_batch_rows, o.hbm_budget = lanes, max_batch_rows, hbm_budget

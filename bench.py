@@ -520,7 +520,7 @@ def run_serve(args, rank, world, local):
         with cuapss.Server(idx, device=local, lanes=3) as srv:
             sweep = []
             with Clocks(local) as clk:
-                for factor in (0.6, 1.5, 3.0, 6.0):
+                for factor in (0.5, 1.0, 2.0, 4.0):
                     reqs = [("query",) + queries(256) for _ in range(args.serve_requests)]
                     rate = factor * 1000.0 / lone_ms
                     infos, wall = drive(srv, reqs, rate)
@@ -604,7 +604,7 @@ def main():
                     choices=["plain_800k", "mixed_1m", "batch", "serve"],
                     help="plain_800k (default); mixed_1m: n = d = 1M; batch: 4,096 instances; "
                          "serve: 5M-vector resident index behind the request server")
-    ap.add_argument("--serve-requests", type=int, default=200)
+    ap.add_argument("--serve-requests", type=int, default=400)
     ap.add_argument("--k", type=int, default=4096, help="instances of the batch workload")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))

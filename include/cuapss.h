@@ -202,7 +202,8 @@ typedef struct cuapss_server cuapss_server;
 
 typedef struct {
   int32_t lanes;           /* batches in flight, default 3 */
-  int64_t max_batch_rows;  /* query rows per batch, default 4096 */
+  int64_t max_batch_rows;  /* query rows per batch, default 1024 (bounds the
+                              time one batch holds the GPU) */
   int64_t hbm_budget;      /* working-memory bytes of batches in flight,
                               default 16 GiB */
 } cuapss_server_opts;
