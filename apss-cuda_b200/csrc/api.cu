@@ -203,6 +203,7 @@ cuapss_status join_device(cuapss_ctx* ctx, const DevCsr& a, const DevCsr* b, flo
         units.push_back(make_int4(I, j0, std::min(je, j0 + chunk), 0));
     }
   }
+  order_units_for_l2(units);
   const int grid = std::max(1, std::min((int)units.size(), grid_max));
   int4* d_units = nullptr;
   ST_TRY(ws.get("tiles:units", std::max<size_t>(units.size(), 1), &d_units));

@@ -223,6 +223,7 @@ cuapss_status prepare_bucket(cuapss_ctx* ctx, const BatchIn& in, Bucket& b, int 
         units.push_back(make_int4(I, j0, std::min(B1, j0 + chunk), 0));
     }
   }
+  order_units_for_l2(units);
   b.nunits = (int)units.size();
   b.grid = std::max(1, std::min(b.nunits, ctx->sms));
   ST_TRY(ws.get(t + "units", std::max<size_t>(units.size(), 1), &b.units));

@@ -426,6 +426,7 @@ cuapss_status cuapss::index_query_rows(cuapss_ctx* ctx, const cuapss_index* idx,
         for (int j0 = 0; j0 < G.nb; j0 += chunk)
           units[s].push_back(make_int4(I, j0, std::min(G.nb, j0 + chunk), 0));
       }
+      order_units_for_l2(units[s]);
       seg_tiles[s] = (int64_t)SQ.nb * G.nb;
       ntiles += seg_tiles[s];
       total_units += units[s].size();

@@ -1,8 +1,10 @@
 // Launch interfaces of the pair-tile kernels and the finalize stage.
 #pragma once
 
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
+#include <vector>
 
 #include "common.cuh"
 #include "side.cuh"
@@ -67,6 +69,23 @@ inline void set_tile_margins(TileArgs& ta, double nrm2, bool mixed) {
                   (ta.p / 16.0 + 2.0) * std::ldexp(1.0, -20) * (1.0 + std::ldexp(1.0, -7));
     ta.eps_head *= 1.001;
   }
+}
+
+// Orders units so that the CTAs running at the same time share operands in
+// L2: units are grouped by the window of J blocks they start in (window =
+// the median J-range length) and ordered by I inside a group. The ~148
+// concurrent units then read a few J blocks (L2 hits) against different I
+// blocks, instead of one I block against 148 different J ranges.
+inline void order_units_for_l2(std::vector<int4>& units) {
+  if (units.size() < 2) return;
+  std::vector<int> len(units.size());
+  for (size_t k = 0; k < units.size(); ++k) len[k] = units[k].z - units[k].y;
+  std::nth_element(len.begin(), len.begin() + len.size() / 2, len.end());
+  const int w = std::max(1, len[len.size() / 2]);
+  std::stable_sort(units.begin(), units.end(), [w](const int4& a, const int4& b) {
+    const int wa = a.y / w, wb = b.y / w;
+    return wa != wb ? wa < wb : a.x < b.x;
+  });
 }
 
 // Plain FP32 hybrid tile kernel (head: FP32 forward-list dot on TMA-staged
