@@ -9,8 +9,8 @@
 // first posting of each feature's run, the run length (8 bits); a table of
 // 4097 bucket offsets (16 bits each) delimits the buckets. Staging is a
 // straight copy plus the offsets: no hashing, no atomics. A block with more
-// than kStagePostings postings is staged in consecutive chunks of
-// kStagePostings postings (any cut is valid: every chunk adds the products
+// postings than the staging capacity is staged in consecutive chunks of that
+// many postings (any cut is valid: every chunk adds the products
 // of its own postings; a run cut by a chunk boundary is re-measured).
 //
 // J side (the columns; one per tile): the tail postings of each 64-row
@@ -34,33 +34,39 @@
 
 namespace cuapss {
 
-constexpr int kStagePostings = 12800;  // postings per staged chunk (16-bit offsets)
-static_assert(kStagePostings < 65536, "bucket offsets are 16 bits");
+constexpr int kStagePostings = 12800;  // default postings per staged chunk (16-bit offsets)
 constexpr uint32_t kMaxTailFeature = (1u << 20) - 1;  // 8-bit tag above 12-bit bucket
 constexpr float kTailScale = 1073741824.0f;              // 2^30
 constexpr float kTailUnscale = 9.313225746154785e-10f;   // 2^-30
 
 constexpr size_t kTailOffBytes = ((size_t)(kTailBuckets + 1) * 2 + 15) / 16 * 16;
-// Shared memory of the staged I postings.
-constexpr size_t kTailStageBytes = kTailOffBytes + (size_t)kStagePostings * 7;
+// Shared memory of CAP staged I postings.
+template <int CAP>
+constexpr size_t tail_stage_bytes() {
+  static_assert(CAP > 0 && CAP < 65536 && CAP % 16 == 0, "bucket offsets are 16 bits");
+  return kTailOffBytes + (size_t)CAP * 7;
+}
+constexpr size_t kTailStageBytes = tail_stage_bytes<kStagePostings>();
 
 __device__ __forceinline__ int tail_fixed(float prod) { return __float2int_rn(prod * kTailScale); }
 
 // Shared-memory staging buffers of the I side.
 struct TailStage {
   uint16_t* boff;  // [kTailBuckets + 1] first posting of each bucket
-  float* eu;       // [kStagePostings] posting: value
-  uint16_t* et;    // [kStagePostings] posting: tag << 7 | row in block
-  uint8_t* en;     // [kStagePostings] run length at a run's first posting
+  float* eu;       // [CAP] posting: value
+  uint16_t* et;    // [CAP] posting: tag << 7 | row in block
+  uint8_t* en;     // [CAP] run length at a run's first posting
 };
 
-// Carves a TailStage out of kTailStageBytes of 16-byte aligned shared memory.
+// Carves a TailStage of CAP postings out of tail_stage_bytes<CAP>() bytes of
+// 16-byte aligned shared memory.
+template <int CAP = kStagePostings>
 __device__ __forceinline__ TailStage tail_stage_at(uint8_t* base) {
   TailStage t;
   t.boff = reinterpret_cast<uint16_t*>(base);
   t.eu = reinterpret_cast<float*>(base + kTailOffBytes);
-  t.et = reinterpret_cast<uint16_t*>(base + kTailOffBytes + (size_t)kStagePostings * 4);
-  t.en = base + kTailOffBytes + (size_t)kStagePostings * 6;
+  t.et = reinterpret_cast<uint16_t*>(base + kTailOffBytes + (size_t)CAP * 4);
+  t.en = base + kTailOffBytes + (size_t)CAP * 6;
   return t;
 }
 
@@ -76,21 +82,22 @@ __device__ __forceinline__ void tail_sync() {
   else named_bar(BAR, NT);
 }
 
-// Chunks of I block I (at least one, possibly empty).
+// Chunks of CAP postings of I block I (at least one, possibly empty).
+template <int CAP = kStagePostings>
 __device__ __forceinline__ int tail_nchunks(const TileArgs& A, int I) {
   const int64_t T = A.bptrI[I + 1] - A.bptrI[I];
-  return T <= kStagePostings ? 1 : (int)((T + kStagePostings - 1) / kStagePostings);
+  return T <= CAP ? 1 : (int)((T + CAP - 1) / CAP);
 }
 
 // Stage chunk c of block I. All NT tail threads (ltid = index among them)
 // call it; it ends with a tail barrier.
-template <int NT, int BAR>
+template <int NT, int BAR, int CAP = kStagePostings>
 __device__ __forceinline__ TailI stage_tail_chunk(const TileArgs& A, const TailStage& S, int I,
                                                   int c, int ltid) {
   const int64_t b1 = A.bptrI[I + 1];
-  const int64_t e0 = A.bptrI[I] + (int64_t)c * kStagePostings;
+  const int64_t e0 = A.bptrI[I] + (int64_t)c * CAP;
   const int64_t rem = b1 - e0;
-  const int P = rem <= 0 ? 0 : (rem < kStagePostings ? (int)rem : kStagePostings);
+  const int P = rem <= 0 ? 0 : (rem < CAP ? (int)rem : CAP);
   TailI T;
   T.P = P;
   T.any = P > 0;

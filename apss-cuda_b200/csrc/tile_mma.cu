@@ -13,7 +13,7 @@
 //
 // Warp roles (one CTA per SM, persistent over a static share of the units):
 //   warp 0       producer: bulk copies of I and J operand tiles into a
-//                kStages-deep shared-memory ring (mbarrier full/empty);
+//                3- or 4-stage shared-memory ring (mbarrier full/empty);
 //   warp 1       MMA: allocates 256 tensor-memory columns (two 128-column
 //                accumulators), one thread issues tcgen05.mma and commits;
 //   warps 2..9   tail + epilogue: the sparse tail of the tile in fixed point
@@ -44,7 +44,6 @@ constexpr int kCT = kCW * 32;                 // their threads
 constexpr int kThreads = 64 + kCT;            // + producer warp + MMA warp
 constexpr int kKC = 64;                       // BF16 features per chunk (128-byte rows)
 constexpr int kTileBytes = kBlockRows * kKC * 2;  // 16 KB per operand chunk
-constexpr int kStages = 3;
 constexpr int kAccCols = 64;                  // tail accumulator: half a tile
 constexpr int kAccLd = kAccCols + 1;          // odd stride: conflict-free row reads
 constexpr uint32_t kTmemCols = 256;
@@ -53,7 +52,7 @@ constexpr int kBatch = 4;                     // J postings per thread per load 
 constexpr int kEpiCols = kAccCols / (kCW / 4);  // tile columns per thread per half (16)
 
 struct SmemM {
-  uint8_t* stage;       // kStages x (A 16 KB | B 16 KB), 1024-byte aligned
+  uint8_t* stage;       // STAGES x (A 16 KB | B 16 KB), 1024-byte aligned
   int* acc;
   float* hnj;
   uint64_t* full;
@@ -68,45 +67,38 @@ struct SmemM {
 
 __host__ __device__ constexpr size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
-struct Layout {
-  size_t acc, hnj, bars, tmem, abort, tail, total;
-  __host__ __device__ constexpr Layout()
-      : acc(0), hnj(0), bars(0), tmem(0), abort(0), tail(0), total(0) {
-    size_t o = (size_t)kStages * 2 * kTileBytes;
-    acc = o;
-    o += (size_t)kBlockRows * kAccLd * 4;
-    hnj = align_up(o, 16);
-    o = hnj + (size_t)kBlockRows * 4;
-    bars = align_up(o, 16);
-    o = bars + (size_t)(2 * kStages + 5) * 8;
-    tmem = align_up(o, 16);
-    o = tmem + 16;
-    abort = o;
-    o += 16;
-    tail = align_up(o, 16);
-    o = tail + kTailStageBytes;
-    total = align_up(o, 16);
-  }
+// Shared-memory layout of the variant with STAGES operand stages and CAP
+// staged tail postings.
+template <int STAGES, int CAP>
+struct Cfg {
+  static constexpr size_t kAcc = (size_t)STAGES * 2 * kTileBytes;
+  static constexpr size_t kHnj = align_up(kAcc + (size_t)kBlockRows * kAccLd * 4, 16);
+  static constexpr size_t kBars = align_up(kHnj + (size_t)kBlockRows * 4, 16);
+  static constexpr size_t kTmem = align_up(kBars + (size_t)(2 * STAGES + 5) * 8, 16);
+  static constexpr size_t kAbort = kTmem + 16;
+  static constexpr size_t kTail = align_up(kAbort + 16, 16);
+  static constexpr size_t kTotal = align_up(kTail + tail_stage_bytes<CAP>(), 16);
+  static constexpr size_t kSmem = kTotal + 1024;  // + alignment slack
+  static_assert(kSmem <= 232448, "shared memory budget");
 };
-constexpr Layout kLayout{};
-constexpr size_t kSmemBytes = kLayout.total + 1024;  // + alignment slack
-static_assert(kSmemBytes <= 232448, "shared memory budget");
 
+template <int STAGES, int CAP>
 __device__ __forceinline__ SmemM carve(uint8_t* raw) {
+  using C = Cfg<STAGES, CAP>;
   uint8_t* base = reinterpret_cast<uint8_t*>(align_up(reinterpret_cast<size_t>(raw), 1024));
   SmemM s;
   s.stage = base;
-  s.acc = reinterpret_cast<int*>(base + kLayout.acc);
-  s.hnj = reinterpret_cast<float*>(base + kLayout.hnj);
-  uint64_t* b = reinterpret_cast<uint64_t*>(base + kLayout.bars);
+  s.acc = reinterpret_cast<int*>(base + C::kAcc);
+  s.hnj = reinterpret_cast<float*>(base + C::kHnj);
+  uint64_t* b = reinterpret_cast<uint64_t*>(base + C::kBars);
   s.full = b;
-  s.empty = b + kStages;
-  s.tfull = b + 2 * kStages;
-  s.tempty = b + 2 * kStages + 2;
-  s.drain = b + 2 * kStages + 4;
-  s.tmem_base = reinterpret_cast<uint32_t*>(base + kLayout.tmem);
-  s.abort = reinterpret_cast<int*>(base + kLayout.abort);
-  s.ts = tail_stage_at(base + kLayout.tail);
+  s.empty = b + STAGES;
+  s.tfull = b + 2 * STAGES;
+  s.tempty = b + 2 * STAGES + 2;
+  s.drain = b + 2 * STAGES + 4;
+  s.tmem_base = reinterpret_cast<uint32_t*>(base + C::kTmem);
+  s.abort = reinterpret_cast<int*>(base + C::kAbort);
+  s.ts = tail_stage_at<CAP>(base + C::kTail);
   return s;
 }
 
@@ -133,13 +125,14 @@ struct MmaArgs {
   int nkc;  // p / 64
 };
 
+template <int STAGES, int CAP>
 __global__ void __launch_bounds__(kThreads, 1) k_tiles_mma(const TileArgs A, const MmaArgs M) {
   extern __shared__ uint8_t smem_raw[];
-  const SmemM S = carve(smem_raw);
+  const SmemM S = carve<STAGES, CAP>(smem_raw);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   volatile int* abort = S.abort;
   if (threadIdx.x == 0) {
-    for (int s = 0; s < kStages; ++s) {
+    for (int s = 0; s < STAGES; ++s) {
       mbar_init(&S.full[s], 1);
       mbar_init(&S.empty[s], 1);
     }
@@ -172,7 +165,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_tiles_mma(const TileArgs A, con
         if (U.y >= U.z) continue;
         for (int J = U.y; ok && J < U.z; ++J) {
           for (int kc = 0; kc < M.nkc; ++kc, ++it) {
-            const uint32_t s = it % kStages, round = it / kStages;
+            const uint32_t s = it % STAGES, round = it / STAGES;
             if (!wait_or_abort(&S.empty[s], (round & 1u) ^ 1u, abort)) {
               raise_abort(A, abort);
               ok = false;
@@ -188,9 +181,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_tiles_mma(const TileArgs A, con
         }
       }
       // drain: the last copies issued must have landed before the CTA exits
-      const uint32_t first = it > (uint32_t)kStages ? it - kStages : 0u;
+      const uint32_t first = it > (uint32_t)STAGES ? it - STAGES : 0u;
       for (uint32_t q = first; q < it; ++q)
-        mbar_wait(&S.full[q % kStages], (q / kStages) & 1u);
+        mbar_wait(&S.full[q % STAGES], (q / STAGES) & 1u);
     }
     __syncwarp();
   } else if (warp == 1) {
@@ -212,7 +205,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_tiles_mma(const TileArgs A, con
           tc_fence_after();
           const uint32_t d = tmem + b * (uint32_t)kBlockRows;
           for (int kc = 0; kc < M.nkc; ++kc, ++it) {
-            const uint32_t s = it % kStages, round = it / kStages;
+            const uint32_t s = it % STAGES, round = it / STAGES;
             if (!wait_or_abort(&S.full[s], round & 1u, abort)) {
               raise_abort(A, abort);
               ok = false;
@@ -252,9 +245,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_tiles_mma(const TileArgs A, con
       const int64_t row0 = (int64_t)I * kBlockRows;
       const int rowsI = (int)(A.nI - row0 < kBlockRows ? A.nI - row0 : kBlockRows);
       named_bar(kComputeBar, kCT);
-      const int nch = tail_nchunks(A, I);
+      const int nch = tail_nchunks<CAP>(A, I);
       TailI T{};
-      if (nch == 1) T = stage_tail_chunk<kCT, kComputeBar>(A, S.ts, I, 0, ctid);
+      if (nch == 1) T = stage_tail_chunk<kCT, kComputeBar, CAP>(A, S.ts, I, 0, ctid);
       const float hn_r = row < rowsI ? A.hnormI[row0 + row] : 0.0f;
       const double t_r = A.t_row ? (row < rowsI ? (double)A.t_row[row0 + row] : 2.0) : (double)A.t;
       for (int J = U.y; ok && J < U.z; ++J, ++tt) {
@@ -275,7 +268,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_tiles_mma(const TileArgs A, con
               tail_postings<kBatch>(A, S.ts, T, k0, k1, S.acc, kAccLd, h * kAccCols, ctid, kCT);
             } else {
               for (int c = 0; c < nch; ++c) {
-                const TailI Tc = stage_tail_chunk<kCT, kComputeBar>(A, S.ts, I, c, ctid);
+                const TailI Tc = stage_tail_chunk<kCT, kComputeBar, CAP>(A, S.ts, I, c, ctid);
                 tail_postings<kBatch>(A, S.ts, Tc, k0, k1, S.acc, kAccLd, h * kAccCols, ctid,
                                       kCT);
                 named_bar(kComputeBar, kCT);  // staging rewritten by the next chunk
@@ -357,7 +350,12 @@ __global__ void __launch_bounds__(kThreads, 1) k_tiles_mma(const TileArgs A, con
 
 }  // namespace
 
-// Opts the kernel into its dynamic shared memory once per device (outside
+// Kernel variants: more operand stages in flight when the I blocks' tails
+// fit a smaller staging area (most inputs), the large staging area otherwise.
+constexpr int kBigStages = 3, kBigCap = 12800;
+constexpr int kSmallStages = 4, kSmallCap = 8192;
+
+// Opts the kernels into their dynamic shared memory once per device (outside
 // any stream capture when called ahead of it).
 cuapss_status tiles_mma_init() {
   static std::mutex mu;
@@ -366,8 +364,12 @@ cuapss_status tiles_mma_init() {
   CU_TRY(cudaGetDevice(&dev));
   std::lock_guard<std::mutex> lk(mu);
   if (dev < 64 && ((done >> dev) & 1ull)) return CUAPSS_OK;
-  CU_TRY(cudaFuncSetAttribute(k_tiles_mma, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)kSmemBytes));
+  CU_TRY(cudaFuncSetAttribute(k_tiles_mma<kBigStages, kBigCap>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)Cfg<kBigStages, kBigCap>::kSmem));
+  CU_TRY(cudaFuncSetAttribute(k_tiles_mma<kSmallStages, kSmallCap>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)Cfg<kSmallStages, kSmallCap>::kSmem));
   if (dev < 64) done |= 1ull << dev;
   return CUAPSS_OK;
 }
@@ -380,11 +382,15 @@ cuapss_status launch_tiles_mma(const TileArgs& a, const void* headI16, const voi
   m.headI16 = static_cast<const uint8_t*>(headI16);
   m.headJ16 = static_cast<const uint8_t*>(headJ16);
   m.nkc = p / kKC;
-  k_tiles_mma<<<grid, kThreads, kSmemBytes, st>>>(a, m);
+  if (a.max_tailI <= kSmallCap)
+    k_tiles_mma<kSmallStages, kSmallCap>
+        <<<grid, kThreads, Cfg<kSmallStages, kSmallCap>::kSmem, st>>>(a, m);
+  else
+    k_tiles_mma<kBigStages, kBigCap><<<grid, kThreads, Cfg<kBigStages, kBigCap>::kSmem, st>>>(a, m);
   LAUNCH_CHECK();
   return CUAPSS_OK;
 }
 
-size_t tiles_mma_smem_bytes() { return kSmemBytes; }
+size_t tiles_mma_smem_bytes() { return Cfg<kBigStages, kBigCap>::kSmem; }
 
 }  // namespace cuapss

@@ -27,6 +27,7 @@ struct TileArgs {
   const uint32_t* bilI_key; // {bucket << 15 | tag << 7 | row}, (bucket, tag, row) order
   const float* bilI_u;
   const uint8_t* bilI_len;  // feature run length at its first posting
+  int64_t max_tailI;        // largest I-block tail (postings): picks the staging variant
   // J side (columns of the tile)
   const float* headJ32;
   const void* headJ16;
