@@ -45,7 +45,7 @@ constexpr int kThreads = 64 + kCT;            // + producer warp + MMA warp
 constexpr int kKC = 64;                       // BF16 features per chunk (128-byte rows)
 constexpr int kTileBytes = kBlockRows * kKC * 2;  // 16 KB per operand chunk
 constexpr int kAccCols = 64;                  // tail accumulator: half a tile
-constexpr int kAccLd = kAccCols + 1;          // odd stride: conflict-free row reads
+constexpr int kAccLd = kAccCols + 4;          // 16-byte rows; 8 rows x 272 B cover all banks
 constexpr uint32_t kTmemCols = 256;
 constexpr int kComputeBar = 1;
 constexpr int kBatch = 4;                     // J postings per thread per load batch
@@ -291,20 +291,28 @@ __global__ void __launch_bounds__(kThreads, 1) k_tiles_mma(const TileArgs A, con
           tmem_ld16(tmem + b * (uint32_t)kBlockRows + (uint32_t)cbase + ((uint32_t)(32 * q) << 16),
                     v);
           uint32_t pass = 0;
-          int* arow = S.acc + row * kAccLd + colq * kEpiCols;
+          int4* arow = reinterpret_cast<int4*>(S.acc + row * kAccLd + colq * kEpiCols);
+          const float4* hn4 = reinterpret_cast<const float4*>(S.hnj + cbase);
           const bool row_ok = row < rowsI;
           const bool simple = !diag && colsJ == kBlockRows;
 #pragma unroll
-          for (int j = 0; j < kEpiCols; ++j) {
-            const int c = cbase + j;
-            const int tq = arow[j];
-            arow[j] = 0;
-            const float s = fmaf(__int2float_rn(tq), kTailUnscale, __uint_as_float(v[j]));
-            v[j] = __float_as_uint(s);
-            const float thr = __fmaf_rd(-hn_r, S.hnj[c], t_lo);
-            bool okp = (s >= thr) && row_ok;
-            if (!simple) okp = okp && (c < colsJ) && (!diag || c > row);
-            pass |= (uint32_t)okp << j;
+          for (int j4 = 0; j4 < kEpiCols / 4; ++j4) {
+            const int4 t4 = arow[j4];
+            arow[j4] = make_int4(0, 0, 0, 0);
+            const float4 h4 = hn4[j4];
+            const int tq[4] = {t4.x, t4.y, t4.z, t4.w};
+            const float hh[4] = {h4.x, h4.y, h4.z, h4.w};
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+              const int j = 4 * j4 + k;
+              const int c = cbase + j;
+              const float s = fmaf(__int2float_rn(tq[k]), kTailUnscale, __uint_as_float(v[j]));
+              v[j] = __float_as_uint(s);
+              const float thr = __fmaf_rd(-hn_r, hh[k], t_lo);
+              bool okp = (s >= thr) && row_ok;
+              if (!simple) okp = okp && (c < colsJ) && (!diag || c > row);
+              pass |= (uint32_t)okp << j;
+            }
           }
           if (__any_sync(0xffffffffu, pass != 0u)) {
             const int mine = __popc(pass);
@@ -352,8 +360,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_tiles_mma(const TileArgs A, con
 
 // Kernel variants: more operand stages in flight when the I blocks' tails
 // fit a smaller staging area (most inputs), the large staging area otherwise.
-constexpr int kBigStages = 3, kBigCap = 12800;
-constexpr int kSmallStages = 4, kSmallCap = 8192;
+constexpr int kBigStages = 3, kBigCap = 12768;
+constexpr int kSmallStages = 4, kSmallCap = 7936;
 
 // Opts the kernels into their dynamic shared memory once per device (outside
 // any stream capture when called ahead of it).
