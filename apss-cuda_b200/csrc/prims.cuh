@@ -136,7 +136,9 @@ static __global__ void __launch_bounds__(kRsThreads) k_rs_upsweep(const uint64_t
 }
 
 // Stable scatter: elements of a tile are ranked in index order (warp w owns
-// elements [w*256, w*256+256) of the tile, in chunks of 32 lanes).
+// elements [w*256, w*256+256) of the tile, in chunks of 32 lanes), placed in
+// shared memory in digit order, then written out so that consecutive threads
+// write consecutive addresses of each digit's run (coalesced stores).
 static __global__ void __launch_bounds__(kRsThreads) k_rs_downsweep(const uint64_t* __restrict__ kin,
                                                              const uint32_t* __restrict__ vin,
                                                              uint64_t* __restrict__ kout,
@@ -144,10 +146,17 @@ static __global__ void __launch_bounds__(kRsThreads) k_rs_downsweep(const uint64
                                                              int shift, const uint32_t* __restrict__ offs,
                                                              int nblocks) {
   __shared__ uint32_t wcnt[kRsWarps][256];
+  __shared__ uint32_t dstart[256];  // first tile slot of each digit
+  __shared__ uint32_t dglob[256];   // first output position of each digit for this tile
+  __shared__ uint32_t wsum[kRsWarps];
+  __shared__ uint64_t skey[kRsTile];
+  __shared__ uint32_t sval[kRsTile];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   for (int i = threadIdx.x; i < kRsWarps * 256; i += kRsThreads) (&wcnt[0][0])[i] = 0;
+  dglob[threadIdx.x] = offs[(int64_t)threadIdx.x * nblocks + blockIdx.x];
   __syncthreads();
-  const int64_t base = (int64_t)blockIdx.x * kRsTile + (int64_t)w * (kRsChunks * 32);
+  const int64_t tile0 = (int64_t)blockIdx.x * kRsTile;
+  const int64_t base = tile0 + (int64_t)w * (kRsChunks * 32);
   uint64_t key[kRsChunks];
   uint32_t val[kRsChunks];
   uint32_t rank[kRsChunks];
@@ -172,7 +181,9 @@ static __global__ void __launch_bounds__(kRsThreads) k_rs_downsweep(const uint64
   }
   __syncthreads();
   {
-    const int d = threadIdx.x;  // kRsThreads == 256 digits
+    // per digit: offsets of the warps inside the digit, then the tile's
+    // exclusive scan over digits (kRsThreads == 256 digits)
+    const int d = threadIdx.x;
     uint32_t run = 0;
 #pragma unroll
     for (int ww = 0; ww < kRsWarps; ++ww) {
@@ -180,6 +191,17 @@ static __global__ void __launch_bounds__(kRsThreads) k_rs_downsweep(const uint64
       wcnt[ww][d] = run;
       run += t;
     }
+    uint32_t x = run;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    if (lane == 31) wsum[w] = x;
+    __syncthreads();
+    uint32_t before = 0;
+    for (int ww = 0; ww < w; ++ww) before += wsum[ww];
+    dstart[d] = before + x - run;
   }
   __syncthreads();
 #pragma unroll
@@ -187,10 +209,19 @@ static __global__ void __launch_bounds__(kRsThreads) k_rs_downsweep(const uint64
     const int64_t idx = base + c * 32 + lane;
     if (idx < n) {
       const unsigned d = (unsigned)(key[c] >> shift) & 255u;
-      const int64_t pos = (int64_t)offs[(int64_t)d * nblocks + blockIdx.x] + wcnt[w][d] + rank[c];
-      kout[pos] = key[c];
-      vout[pos] = val[c];
+      const uint32_t lp = dstart[d] + wcnt[w][d] + rank[c];
+      skey[lp] = key[c];
+      sval[lp] = val[c];
     }
+  }
+  __syncthreads();
+  const int tile_n = (int)(n - tile0 < kRsTile ? n - tile0 : kRsTile);
+  for (int i = threadIdx.x; i < tile_n; i += kRsThreads) {
+    const uint64_t k = skey[i];
+    const unsigned d = (unsigned)(k >> shift) & 255u;
+    const int64_t pos = (int64_t)dglob[d] + (i - (int)dstart[d]);
+    kout[pos] = k;
+    vout[pos] = sval[i];
   }
 }
 
