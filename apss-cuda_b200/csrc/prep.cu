@@ -19,6 +19,7 @@
 
 #include <algorithm>
 #include <cstring>
+#include <mutex>
 
 #include "prep.cuh"
 #include "prims.cuh"
@@ -59,12 +60,25 @@ __global__ void k_check_rowptr(const int64_t* __restrict__ rp, int64_t n, int64_
 }
 
 // One warp per row: id range/order, finite values, FP64 norm, posting counts.
+// Posting counts of up to kHistMax features are first gathered in a per-CTA
+// shared-memory histogram (hot Zipf features would otherwise serialize on
+// one global counter), then added to counts once per CTA.
+constexpr int64_t kHistMax = 50176;
+
+template <bool SMEM_HIST>
 __global__ void k_check_rows(const int64_t* __restrict__ rp, const int32_t* __restrict__ col,
                              const float* __restrict__ val, int64_t n, int64_t d, float tol,
                              int check, int32_t* __restrict__ counts, int* err,
                              unsigned long long* nrm_max_bits) {
+  extern __shared__ int hist[];
+  if (SMEM_HIST) {
+    for (int64_t f = threadIdx.x; f < d; f += blockDim.x) hist[f] = 0;
+    __syncthreads();
+  }
   const int lane = threadIdx.x & 31;
   const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  double nrm_max = 0.0;  // this warp's rows (one global atomic per warp at the end)
+  int bad_all = 0;
   for (int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; i < n; i += warps) {
     const int64_t lo = rp[i], hi = rp[i + 1];
     double ss = 0.0;
@@ -76,17 +90,27 @@ __global__ void k_check_rows(const int64_t* __restrict__ rp, const int32_t* __re
       if (e > lo && col[e - 1] >= c) bad |= kErrColOrder;
       if (!isfinite(v)) bad |= kErrValue;
       ss += (double)v * (double)v;
-      if (counts && c >= 0 && c < d) atomicAdd(&counts[c], 1);
+      if (counts && c >= 0 && c < d) {
+        if (SMEM_HIST) atomicAdd(&hist[c], 1);
+        else atomicAdd(&counts[c], 1);
+      }
     }
     ss = warp_sum_d(ss);
     bad = warp_or(bad);
-    if (lane == 0) {
-      const double nrm = sqrt(ss);
-      if (check && hi > lo && fabs(nrm - 1.0) > (double)tol) bad |= kErrNorm;
-      if (!check) bad &= ~kErrNorm;
-      if (bad) atomicOr(err, bad);
-      atomicMax(nrm_max_bits, (unsigned long long)__double_as_longlong(nrm));
-    }
+    const double nrm = sqrt(ss);
+    if (check && hi > lo && fabs(nrm - 1.0) > (double)tol) bad |= kErrNorm;
+    bad_all |= bad;
+    nrm_max = fmax(nrm_max, nrm);
+  }
+  if (lane == 0) {
+    if (bad_all) atomicOr(err, bad_all);
+    if (nrm_max > 0.0) atomicMax(nrm_max_bits, (unsigned long long)__double_as_longlong(nrm_max));
+  }
+  if (SMEM_HIST) {
+    __syncthreads();
+    if (counts)
+      for (int64_t f = threadIdx.x; f < d; f += blockDim.x)
+        if (hist[f]) atomicAdd(&counts[f], hist[f]);
   }
 }
 
@@ -388,8 +412,28 @@ cuapss_status validate_csr(const int64_t* rp, const int32_t* col, const float* v
   CU_TRY(cudaMemcpyAsync(&h_err, err, sizeof(int), cudaMemcpyDeviceToHost, st));
   CU_TRY(cudaStreamSynchronize(st));
   if (h_err) return CUAPSS_EINVAL;
-  k_check_rows<<<grid_for(n * 32, kThreads), kThreads, 0, st>>>(rp, col, val, n, d, tol, check,
-                                                                counts, err, nm);
+  if (counts && d <= kHistMax && nnz >= 4 * d) {
+    static std::mutex mu;
+    static uint64_t done = 0;  // attribute set, bit per device
+    int dev = 0;
+    CU_TRY(cudaGetDevice(&dev));
+    {
+      std::lock_guard<std::mutex> lk(mu);
+      if (dev >= 64 || !((done >> dev) & 1ull)) {
+        CU_TRY(cudaFuncSetAttribute(k_check_rows<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)(kHistMax * sizeof(int))));
+        if (dev < 64) done |= 1ull << dev;
+      }
+    }
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const unsigned g = (unsigned)std::max<int64_t>(1, std::min<int64_t>(sms, ceil_div(n, 32)));
+    k_check_rows<true><<<g, 1024, (size_t)d * sizeof(int), st>>>(rp, col, val, n, d, tol, check,
+                                                                  counts, err, nm);
+  } else {
+    k_check_rows<false><<<grid_for(n * 32, kThreads), kThreads, 0, st>>>(rp, col, val, n, d, tol,
+                                                                       check, counts, err, nm);
+  }
   LAUNCH_CHECK();
   unsigned long long h_nm = 0;
   CU_TRY(cudaMemcpyAsync(&h_err, err, sizeof(int), cudaMemcpyDeviceToHost, st));
