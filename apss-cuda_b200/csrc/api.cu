@@ -93,7 +93,8 @@ float elapsed(cudaEvent_t a, cudaEvent_t b) {
 }  // namespace
 
 cuapss_status join_device(cuapss_ctx* ctx, const DevCsr& a, const DevCsr* b, float t,
-                          cuapss_pairs* out, cuapss_stats* stats) {
+                          cuapss_pairs* out, cuapss_stats* stats, int shard, int nshards) {
+  if (nshards < 1 || shard < 0 || shard >= nshards) return CUAPSS_EINVAL;
   const bool self = (b == nullptr);
   const DevCsr& bb = self ? a : *b;
   if (!self && a.d != bb.d) return CUAPSS_EINVAL;
@@ -194,10 +195,11 @@ cuapss_status join_device(cuapss_ctx* ctx, const DevCsr& a, const DevCsr* b, flo
     auto weight = [&](int I) {
       return 1.0 + (double)(SA.h_bptr[I + 1] - SA.h_bptr[I]) / avg;
     };
+    // a shard takes the I blocks with I mod nshards == shard
     double total = 0.0;
-    for (int I = 0; I < SA.nb; ++I) total += weight(I) * (SJ->nb - (self ? I : 0));
+    for (int I = shard; I < SA.nb; I += nshards) total += weight(I) * (SJ->nb - (self ? I : 0));
     const double target = std::max(1.0, total / (grid_max * 16.0));
-    for (int I = 0; I < SA.nb; ++I) {
+    for (int I = shard; I < SA.nb; I += nshards) {
       const int jb = self ? I : 0, je = SJ->nb;
       const int chunk = (int)std::max(1.0, std::floor(target / weight(I)));
       for (int j0 = jb; j0 < je; j0 += chunk)
@@ -224,7 +226,8 @@ cuapss_status join_device(cuapss_ctx* ctx, const DevCsr& a, const DevCsr* b, flo
   ta.err = err;
   ta.cand_count = ccount;
   if (ctx->cand_cap == 0) ctx->cand_cap = std::max<int64_t>(1 << 20, 8 * (a.n + bb.n));
-  const int64_t ntiles = self ? (int64_t)SA.nb * (SA.nb + 1) / 2 : (int64_t)SA.nb * SJ->nb;
+  int64_t ntiles = 0;
+  for (const int4& u : units) ntiles += u.z - u.y;
   for (int attempt = 0; attempt < 3; ++attempt) {
     ST_TRY(ws.get("cand:key", (size_t)ctx->cand_cap, &ta.cand_key));
     ST_TRY(ws.get("cand:sim", (size_t)ctx->cand_cap, &ta.cand_sim));
@@ -427,6 +430,25 @@ cuapss_status cuapss_run(cuapss_ctx* c, const cuapss_csr* x, float t, cuapss_pai
   DevCsr a;
   ST_TRY(stage_csr(c, x, "X", &a));
   return join_device(c, a, nullptr, t, out, stats);
+}
+
+cuapss_status cuapss_run_shard(cuapss_ctx* c, const cuapss_csr* x, float t, int32_t shard,
+                               int32_t nshards, cuapss_pairs* out, cuapss_stats* stats) {
+  if (!c) return CUAPSS_EINVAL;
+  CU_TRY(cudaSetDevice(c->device));
+  DevCsr a;
+  ST_TRY(stage_csr(c, x, "X", &a));
+  return join_device(c, a, nullptr, t, out, stats, shard, nshards);
+}
+
+int32_t cuapss_shard_blocks(int64_t n, int32_t shard, int32_t nshards, int32_t* blocks,
+                            int64_t capacity) {
+  if (n < 0 || nshards < 1 || shard < 0 || shard >= nshards) return -1;
+  const int64_t nb = (n + kBlockRows - 1) / kBlockRows;
+  int64_t k = 0;
+  for (int64_t b = shard; b < nb; b += nshards, ++k)
+    if (blocks && k < capacity) blocks[k] = (int32_t)b;
+  return (int32_t)k;
 }
 
 cuapss_status cuapss_join(cuapss_ctx* c, const cuapss_csr* a, const cuapss_csr* b, float t,

@@ -42,7 +42,8 @@ cuapss_status stage_csr(cuapss_ctx* ctx, const cuapss_csr* x, const std::string&
 
 // The self-join (b == nullptr) or cross-join of staged matrices.
 cuapss_status join_device(cuapss_ctx* ctx, const DevCsr& a, const DevCsr* b, float t,
-                          cuapss_pairs* out, cuapss_stats* stats);
+                          cuapss_pairs* out, cuapss_stats* stats, int shard = 0,
+                          int nshards = 1);
 
 // Head width used when the options leave it to the library.
 int choose_head_width(int precision, int64_t n, int64_t d, int64_t nnz);

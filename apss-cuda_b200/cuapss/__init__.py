@@ -114,7 +114,7 @@ class RequestInfo(ctypes.Structure):
 EXPORTED = [
     "cuapss_default_opts", "cuapss_status_string", "cuapss_abi_version", "cuapss_create",
     "cuapss_destroy", "cuapss_run", "cuapss_join", "cuapss_build_index", "cuapss_feature_remap",
-    "cuapss_batch_run", "cuapss_index_create", "cuapss_index_append", "cuapss_index_query",
+    "cuapss_batch_run", "cuapss_run_shard", "cuapss_shard_blocks", "cuapss_index_create", "cuapss_index_append", "cuapss_index_query",
     "cuapss_index_info", "cuapss_index_destroy", "cuapss_server_default_opts",
     "cuapss_server_create", "cuapss_server_submit_query", "cuapss_server_submit_append",
     "cuapss_server_wait", "cuapss_server_destroy",
@@ -152,6 +152,13 @@ def lib():
         L.cuapss_batch_run.argtypes = [_P, ctypes.POINTER(CsrDesc), ctypes.c_int32, _P, _P,
                                        ctypes.POINTER(PairsDesc), ctypes.POINTER(Stats), _P]
         L.cuapss_batch_run.restype = ctypes.c_int
+        L.cuapss_run_shard.argtypes = [_P, ctypes.POINTER(CsrDesc), ctypes.c_float, ctypes.c_int32,
+                                       ctypes.c_int32, ctypes.POINTER(PairsDesc),
+                                       ctypes.POINTER(Stats)]
+        L.cuapss_run_shard.restype = ctypes.c_int
+        L.cuapss_shard_blocks.argtypes = [ctypes.c_int64, ctypes.c_int32, ctypes.c_int32, _P,
+                                          ctypes.c_int64]
+        L.cuapss_shard_blocks.restype = ctypes.c_int32
         L.cuapss_index_create.argtypes = [_P, ctypes.POINTER(CsrDesc), ctypes.POINTER(_P)]
         L.cuapss_index_create.restype = ctypes.c_int
         L.cuapss_index_append.argtypes = [_P, _P, ctypes.POINTER(CsrDesc)]
@@ -269,6 +276,29 @@ class Context:
         """Self-join: (i, j, sim) numpy arrays, i < j, sorted by (i, j)."""
         d, keep = _desc(x)
         return self._pairs_call(lib().cuapss_run, (ctypes.byref(d), ctypes.c_float(t)), capacity)
+
+    def run_shard(self, x, t: float, shard: int, nshards: int, capacity: int = 1 << 16):
+        """One shard of run(): pairs whose row i lies in a 128-row block b with
+        b % nshards == shard; the shards' union is run()'s output."""
+        d, keep = _desc(x)
+        return self._pairs_call(lib().cuapss_run_shard,
+                                (ctypes.byref(d), ctypes.c_float(t), int(shard), int(nshards)),
+                                capacity)
+
+    def run_shard_device(self, x, t: float, shard: int, nshards: int, out: dict):
+        """run_shard into CUDA tensors out = {"i", "j", "sim"}; returns the
+        pair count (raises CuapssError(EOVERFLOW) with self.required set)."""
+        d, keep = _desc(x)
+        cap = int(out["i"].numel())
+        pr = PairsDesc(out["i"].data_ptr(), out["j"].data_ptr(), out["sim"].data_ptr(), cap, 0, 1)
+        st = Stats()
+        s = lib().cuapss_run_shard(self._h, ctypes.byref(d), ctypes.c_float(t), int(shard),
+                                   int(nshards), ctypes.byref(pr), ctypes.byref(st))
+        self.last_stats = st.as_dict()
+        if s == EOVERFLOW:
+            self.required = int(pr.count)
+        _check(s, "cuapss_run_shard")
+        return int(pr.count)
 
     def run_device(self, x, t: float, out: dict):
         """Self-join into CUDA tensors out = {"i", "j", "sim"}; returns the
@@ -493,3 +523,13 @@ class Server:
             self.close()
         except Exception:
             pass
+
+
+def shard_blocks(n: int, shard: int, nshards: int) -> np.ndarray:
+    """Row blocks (128 rows each) of an n-row self-join owned by a shard."""
+    m = lib().cuapss_shard_blocks(int(n), int(shard), int(nshards), None, 0)
+    if m < 0:
+        raise ValueError("bad shard arguments")
+    out = np.empty(max(m, 1), np.int32)
+    lib().cuapss_shard_blocks(int(n), int(shard), int(nshards), out.ctypes.data, m)
+    return out[:m]

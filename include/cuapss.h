@@ -134,6 +134,23 @@ cuapss_status cuapss_destroy(cuapss_ctx* ctx);
 cuapss_status cuapss_run(cuapss_ctx* ctx, const cuapss_csr* x, float t,
                          cuapss_pairs* out, cuapss_stats* stats);
 
+/* One shard of cuapss_run, for one process per GPU with no exchange between
+ * them: the pairs (i, j), i < j, of the self-join whose row i lies in a
+ * 128-row block b = i / 128 with b mod nshards == shard. The shards of
+ * 0..nshards-1 are disjoint and their union is cuapss_run's output; every
+ * shard prepares the whole matrix and evaluates about 1/nshards of the pair
+ * tiles. The reference splits its input into 8 fixed partitions and joins
+ * them one after another on one GPU (similarity_search.cu:1273-2993). */
+cuapss_status cuapss_run_shard(cuapss_ctx* ctx, const cuapss_csr* x, float t,
+                               int32_t shard, int32_t nshards, cuapss_pairs* out,
+                               cuapss_stats* stats);
+
+/* Row blocks owned by a shard of an n-row self-join (host only): writes up
+ * to `capacity` block indices to blocks (may be NULL) and returns how many
+ * there are, or -1 for bad arguments. */
+int32_t cuapss_shard_blocks(int64_t n, int32_t shard, int32_t nshards, int32_t* blocks,
+                            int64_t capacity);
+
 /* Cross-join: all pairs (a, b), a row of `a`, b row of `b`, sim >= t.
  * out->i holds the row of `a`, out->j the row of `b`; sorted by (i, j).
  * This is the per-partition-pair join of the reference
