@@ -46,17 +46,31 @@ inline unsigned grid_for(int64_t work, int threads) {
   return (unsigned)std::min<int64_t>(g, 148 * 16);
 }
 
-// Exact-size device allocations owned by one object.
+// Exact-size device allocations owned by one object, stream-ordered: taken
+// with cudaMallocAsync on the building stream and returned with
+// cudaFreeAsync on the index's own stream, so that neither stalls the other
+// streams' work (cudaMalloc / cudaFree can synchronize the whole device).
 class DevHeap {
  public:
+  explicit DevHeap(cudaStream_t free_stream = nullptr) : free_st_(free_stream) {}
   ~DevHeap() {
-    for (void* p : ptrs_) cudaFree(p);
+    for (void* p : ptrs_) {
+      if (free_st_) cudaFreeAsync(p, free_st_);
+      else cudaFree(p);
+    }
+  }
+  DevHeap(const DevHeap&) = delete;
+  DevHeap& operator=(const DevHeap&) = delete;
+  void set_streams(cudaStream_t alloc_stream, cudaStream_t free_stream) {
+    alloc_st_ = alloc_stream;
+    free_st_ = free_stream;
   }
   template <typename T>
   cuapss_status alloc(size_t count, T** out) {
     void* p = nullptr;
     const size_t bytes = std::max<size_t>(count * sizeof(T), 256);
-    if (cudaMalloc(&p, bytes) != cudaSuccess) {
+    const cudaError_t e = alloc_st_ ? cudaMallocAsync(&p, bytes, alloc_st_) : cudaMalloc(&p, bytes);
+    if (e != cudaSuccess) {
       cudaGetLastError();
       return CUAPSS_ENOMEM;
     }
@@ -78,6 +92,8 @@ class DevHeap {
  private:
   std::vector<void*> ptrs_;
   size_t bytes_ = 0;
+  cudaStream_t alloc_st_ = nullptr;
+  cudaStream_t free_st_ = nullptr;
 };
 
 // One immutable run of index rows and its J-side arrays.
@@ -117,7 +133,15 @@ __global__ void k_concat_rowptr(const int64_t* __restrict__ a, int64_t na,
 }  // namespace cuapss
 
 struct cuapss_index {
+  ~cuapss_index() {
+    segs.clear();  // their memory goes back on free_st
+    if (free_st) {
+      cudaStreamSynchronize(free_st);
+      cudaStreamDestroy(free_st);
+    }
+  }
   int device = 0;
+  cudaStream_t free_st = nullptr;  // stream-ordered frees of dropped segments
   bool mixed = false;
   int p = 0;
   int64_t d = 0;
@@ -140,6 +164,7 @@ cuapss_status build_segment(cuapss_ctx* ctx, const cuapss_index* idx, const DevC
                             int64_t row0, double nrm, std::shared_ptr<Segment>* out) {
   cudaStream_t st = ctx->stream;
   auto seg = std::make_shared<Segment>();
+  seg->heap.set_streams(st, idx->free_st);
   seg->row0 = row0;
   seg->n = x.n;
   seg->nnz = x.nnz;
@@ -242,6 +267,16 @@ extern "C" cuapss_status cuapss_index_create(cuapss_ctx* ctx, const cuapss_csr* 
   ST_TRY(stage_csr(ctx, x, "IX", &a));
   auto idx = std::make_unique<cuapss_index>();
   idx->device = ctx->device;
+  CU_TRY(cudaStreamCreateWithFlags(&idx->free_st, cudaStreamNonBlocking));
+  {
+    // keep freed segment memory in the device's pool for the next segments
+    cudaMemPool_t pool = nullptr;
+    if (cudaDeviceGetDefaultMemPool(&pool, ctx->device) == cudaSuccess) {
+      uint64_t keep = UINT64_MAX;
+      cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+    cudaGetLastError();
+  }
   idx->mixed = ctx->opts.precision == CUAPSS_PREC_MIXED;
   idx->d = a.d;
   idx->norm_tol = ctx->opts.norm_tol;
@@ -309,8 +344,8 @@ extern "C" cuapss_status cuapss_index_append(cuapss_ctx* ctx, cuapss_index* idx,
     segs.pop_back();
     segs.push_back(merged);
   }
-  ctx->ws.release_prefix("seg:");
-  ctx->ws.release_prefix("merge:");
+  // the build temporaries stay in ctx's grow-only workspace: freeing them
+  // here would synchronize the device under running queries
   {
     std::lock_guard<std::mutex> lk(idx->mu);
     idx->segs = segs;

@@ -521,6 +521,10 @@ def run_serve(args, rank, world, local):
         # scenario A: 256-query requests at offered loads relative to the
         # lone service rate (1.0 = one request in flight at a time)
         with cuapss.Server(idx, device=local, lanes=3) as srv:
+            # warm-up: every lane's first batches grow its working memory
+            warm = [srv.submit_query(*queries(1024)) for _ in range(9)]
+            for tk in warm:
+                srv.wait(tk, capacity=1 << 20)
             sweep = []
             with Clocks(local) as clk:
                 for factor in (0.5, 1.0, 2.0, 4.0):
