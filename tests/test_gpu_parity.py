@@ -213,3 +213,34 @@ def test_scale_sampled_rows(gpu_ctx):
     k = np.arange(0, len(gi), max(1, len(gi) // 5000))
     s64 = oracle.pair_sims(x, gi[k], gj[k])
     assert np.max(np.abs(gs[k] - s64)) <= SIM_TOL and np.all(s64 >= t)
+
+
+@pytest.mark.parametrize("precision", [cuapss.PREC_MIXED, cuapss.PREC_FP32], ids=["mixed", "fp32"])
+def test_row_lengths_across_sort_paths(precision):
+    # rows of 1..32 entries (warp sort), 33..4096 (block sort) and > 4096
+    # (the global sort fallback), with near-duplicates of the long rows
+    rng = np.random.default_rng(7)
+    d = 12_000
+    lens = [1, 2, 31, 32, 33, 64, 65, 1000, 4096, 4097, 6000]
+    rows = []
+    for L in lens:
+        f = np.sort(rng.choice(d, size=L, replace=False)).astype(np.int32)
+        v = rng.uniform(0.5, 1.5, size=L)
+        rows.append((f, v))
+        g = f.copy()
+        w = v * rng.uniform(0.95, 1.05, size=L)
+        rows.append((g, w))  # a near-duplicate of it
+    for _ in range(200):
+        L = int(rng.integers(1, 80))
+        rows.append((np.sort(rng.choice(d, size=L, replace=False)).astype(np.int32),
+                     rng.uniform(0.5, 1.5, size=L)))
+    rp = np.zeros(len(rows) + 1, np.int64)
+    rp[1:] = np.cumsum([len(f) for f, _ in rows])
+    col = np.concatenate([f for f, _ in rows])
+    val = np.concatenate([(v / np.linalg.norm(v)) for _, v in rows]).astype(np.float32)
+    x = synth.Csr(rp, col, val, d)
+    with cuapss.Context(precision=precision) as c:
+        for t in (0.3, 0.9):
+            got = c.run(x, t)
+            _check_pairs(got, oracle.apss(x, t))
+            assert got[0].size > 0
