@@ -16,10 +16,11 @@
 //                3- or 4-stage shared-memory ring (mbarrier full/empty);
 //   warp 1       MMA: allocates 256 tensor-memory columns (two 128-column
 //                accumulators), one thread issues tcgen05.mma and commits;
-//   warps 2..9   tail + epilogue: the sparse tail of the tile in fixed point
-//                (tail.cuh), in two 64-column halves, then the accumulator is
-//                read with tcgen05.ld, head + tail is compared with
-//                t - eps(i, j) and candidates are compacted with a warp ballot.
+//   warps 2..25  tail: the sparse tail of the tile in fixed point
+//                (tail.cuh), in two 64-column halves; the first 16 of them
+//                then run the epilogue: the accumulator is read with
+//                tcgen05.ld, head + tail is compared with t - eps(i, j) and
+//                candidates are compacted with a warp ballot.
 // eps(i, j) bounds BF16 input rounding (2^-8 relative per factor) and the
 // FP32 / fixed-point sums, so no pair with FP64 similarity >= t is dropped;
 // the finalize stage decides the band exactly in FP64.
@@ -39,7 +40,8 @@ namespace cuapss {
 
 namespace {
 
-constexpr int kCW = 16;                       // tail + epilogue warps (4 per lane quarter)
+constexpr int kCW = 24;                       // tail warps; the first kEpiW also run the epilogue
+constexpr int kEpiW = 16;                     // epilogue warps (4 per tensor-memory lane quarter)
 constexpr int kCT = kCW * 32;                 // their threads
 constexpr int kThreads = 64 + kCT;            // + producer warp + MMA warp
 constexpr int kKC = 64;                       // BF16 features per chunk (128-byte rows)
@@ -49,7 +51,7 @@ constexpr int kAccLd = kAccCols + 4;          // 16-byte rows; 8 rows x 272 B co
 constexpr uint32_t kTmemCols = 256;
 constexpr int kComputeBar = 1;
 constexpr int kBatch = 4;                     // J postings per thread per load batch
-constexpr int kEpiCols = kAccCols / (kCW / 4);  // tile columns per thread per half (16)
+constexpr int kEpiCols = kAccCols / (kEpiW / 4);  // tile columns per thread per half (16)
 
 struct SmemM {
   uint8_t* stage;       // STAGES x (A 16 KB | B 16 KB), 1024-byte aligned
@@ -138,7 +140,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_tiles_mma(const TileArgs A, con
     }
     for (int b = 0; b < 2; ++b) {
       mbar_init(&S.tfull[b], 1);
-      mbar_init(&S.tempty[b], kCW);
+      mbar_init(&S.tempty[b], kEpiW);
     }
     mbar_init(S.drain, 1);
     *abort = 0;
@@ -233,6 +235,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_tiles_mma(const TileArgs A, con
   } else {
     // ---------------------------------------------- tail + epilogue warps
     const int ctid = threadIdx.x - 64;
+    const bool epi = (warp - 2) < kEpiW;  // this warp also runs the epilogue
     const int q = warp & 3;             // tensor-memory lane quarter of this warp
     const int colq = (warp - 2) >> 2;   // which kEpiCols of each 64 columns
     const int row = 32 * q + lane;
@@ -285,57 +288,59 @@ __global__ void __launch_bounds__(kThreads, 1) k_tiles_mma(const TileArgs A, con
             }
             tc_fence_after();
           }
-          // ---- epilogue: head (tensor memory) + tail (shared) vs t - eps
-          const int cbase = h * kAccCols + colq * kEpiCols;  // first tile column of this thread
-          uint32_t v[kEpiCols];
-          tmem_ld16(tmem + b * (uint32_t)kBlockRows + (uint32_t)cbase + ((uint32_t)(32 * q) << 16),
-                    v);
-          uint32_t pass = 0;
-          int4* arow = reinterpret_cast<int4*>(S.acc + row * kAccLd + colq * kEpiCols);
-          const float4* hn4 = reinterpret_cast<const float4*>(S.hnj + cbase);
-          const bool row_ok = row < rowsI;
-          const bool simple = !diag && colsJ == kBlockRows;
-#pragma unroll
-          for (int j4 = 0; j4 < kEpiCols / 4; ++j4) {
-            const int4 t4 = arow[j4];
-            arow[j4] = make_int4(0, 0, 0, 0);
-            const float4 h4 = hn4[j4];
-            const int tq[4] = {t4.x, t4.y, t4.z, t4.w};
-            const float hh[4] = {h4.x, h4.y, h4.z, h4.w};
-#pragma unroll
-            for (int k = 0; k < 4; ++k) {
-              const int j = 4 * j4 + k;
-              const int c = cbase + j;
-              const float s = fmaf(__int2float_rn(tq[k]), kTailUnscale, __uint_as_float(v[j]));
-              v[j] = __float_as_uint(s);
-              const float thr = __fmaf_rd(-hn_r, hh[k], t_lo);
-              bool okp = (s >= thr) && row_ok;
-              if (!simple) okp = okp && (c < colsJ) && (!diag || c > row);
-              pass |= (uint32_t)okp << j;
+          if (epi) {
+            // ---- epilogue: head (tensor memory) + tail (shared) vs t - eps
+            const int cbase = h * kAccCols + colq * kEpiCols;  // first tile column of this thread
+            uint32_t v[kEpiCols];
+            tmem_ld16(
+                tmem + b * (uint32_t)kBlockRows + (uint32_t)cbase + ((uint32_t)(32 * q) << 16), v);
+            uint32_t pass = 0;
+            int4* arow = reinterpret_cast<int4*>(S.acc + row * kAccLd + colq * kEpiCols);
+            const float4* hn4 = reinterpret_cast<const float4*>(S.hnj + cbase);
+            const bool row_ok = row < rowsI;
+            const bool simple = !diag && colsJ == kBlockRows;
+  #pragma unroll
+            for (int j4 = 0; j4 < kEpiCols / 4; ++j4) {
+              const int4 t4 = arow[j4];
+              arow[j4] = make_int4(0, 0, 0, 0);
+              const float4 h4 = hn4[j4];
+              const int tq[4] = {t4.x, t4.y, t4.z, t4.w};
+              const float hh[4] = {h4.x, h4.y, h4.z, h4.w};
+  #pragma unroll
+              for (int k = 0; k < 4; ++k) {
+                const int j = 4 * j4 + k;
+                const int c = cbase + j;
+                const float s = fmaf(__int2float_rn(tq[k]), kTailUnscale, __uint_as_float(v[j]));
+                v[j] = __float_as_uint(s);
+                const float thr = __fmaf_rd(-hn_r, hh[k], t_lo);
+                bool okp = (s >= thr) && row_ok;
+                if (!simple) okp = okp && (c < colsJ) && (!diag || c > row);
+                pass |= (uint32_t)okp << j;
+              }
             }
-          }
-          if (__any_sync(0xffffffffu, pass != 0u)) {
-            const int mine = __popc(pass);
-            int incl = mine;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-              const int x = __shfl_up_sync(0xffffffffu, incl, o);
-              if (lane >= o) incl += x;
-            }
-            const int total = __shfl_sync(0xffffffffu, incl, 31);
-            unsigned long long base = 0;
-            if (lane == 31) base = atomicAdd(A.cand_count, (unsigned long long)total);
-            base = __shfl_sync(0xffffffffu, base, 31);
-            unsigned long long w = base + (unsigned long long)(incl - mine);
-#pragma unroll
-            for (int j = 0; j < kEpiCols; ++j) {
-              if ((pass >> j) & 1u) {
-                if ((int64_t)w < A.cand_cap) {
-                  A.cand_key[w] =
-                      ((uint64_t)(row0 + row) << 32) | (uint64_t)(col0 + cbase + j);
-                  A.cand_sim[w] = __uint_as_float(v[j]);
+            if (__any_sync(0xffffffffu, pass != 0u)) {
+              const int mine = __popc(pass);
+              int incl = mine;
+  #pragma unroll
+              for (int o = 1; o < 32; o <<= 1) {
+                const int x = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += x;
+              }
+              const int total = __shfl_sync(0xffffffffu, incl, 31);
+              unsigned long long base = 0;
+              if (lane == 31) base = atomicAdd(A.cand_count, (unsigned long long)total);
+              base = __shfl_sync(0xffffffffu, base, 31);
+              unsigned long long w = base + (unsigned long long)(incl - mine);
+  #pragma unroll
+              for (int j = 0; j < kEpiCols; ++j) {
+                if ((pass >> j) & 1u) {
+                  if ((int64_t)w < A.cand_cap) {
+                    A.cand_key[w] =
+                        ((uint64_t)(row0 + row) << 32) | (uint64_t)(col0 + cbase + j);
+                    A.cand_sim[w] = __uint_as_float(v[j]);
+                  }
+                  ++w;
                 }
-                ++w;
               }
             }
           }
@@ -344,7 +349,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_tiles_mma(const TileArgs A, con
         if (!ok) break;
         tc_fence_before();
         __syncwarp();
-        if (lane == 0) mbar_arrive(&S.tempty[b]);
+        if (lane == 0 && epi) mbar_arrive(&S.tempty[b]);
       }
     }
   }
