@@ -16,7 +16,7 @@
 //                3- or 4-stage shared-memory ring (mbarrier full/empty);
 //   warp 1       MMA: allocates 256 tensor-memory columns (two 128-column
 //                accumulators), one thread issues tcgen05.mma and commits;
-//   warps 2..25  tail: the sparse tail of the tile in fixed point
+//   warps 2..31  tail: the sparse tail of the tile in fixed point
 //                (tail.cuh), in two 64-column halves; the first 16 of them
 //                then run the epilogue: the accumulator is read with
 //                tcgen05.ld, head + tail is compared with t - eps(i, j) and
@@ -40,7 +40,7 @@ namespace cuapss {
 
 namespace {
 
-constexpr int kCW = 24;                       // tail warps; the first kEpiW also run the epilogue
+constexpr int kCW = 30;                       // tail warps; the first kEpiW also run the epilogue
 constexpr int kEpiW = 16;                     // epilogue warps (4 per tensor-memory lane quarter)
 constexpr int kCT = kCW * 32;                 // their threads
 constexpr int kThreads = 64 + kCT;            // + producer warp + MMA warp
