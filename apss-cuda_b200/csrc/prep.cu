@@ -174,6 +174,40 @@ __global__ void k_entry_keys(const int64_t* __restrict__ rp, const int32_t* __re
   }
 }
 
+// Remapped ids of each row split into its head (rank < p, written forward
+// from the row's start) and its tail (written backward from its end), one
+// warp per row, rows in input order. Nothing downstream depends on the order
+// inside either part: the head block is a dense scatter, and the tail lists
+// are built by stable sorts on (block, feature) / (half-block, feature), which
+// see the rows in order.
+__global__ void k_split_rows(const int64_t* __restrict__ rp, const int32_t* __restrict__ col,
+                             const float* __restrict__ val, const int32_t* __restrict__ perm,
+                             int64_t n, int p, int32_t* __restrict__ col2,
+                             float* __restrict__ val2) {
+  const int lane = threadIdx.x & 31;
+  const unsigned lt = (1u << lane) - 1u;
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; i < n; i += warps) {
+    const int64_t lo = rp[i], hi = rp[i + 1];
+    int64_t nh = 0, nt = 0;
+    for (int64_t base = lo; base < hi; base += 32) {
+      const int64_t e = base + lane;
+      const bool valid = e < hi;
+      const int32_t rank = valid ? perm[col[e]] : 0;
+      const float v = valid ? val[e] : 0.0f;
+      const unsigned hb = __ballot_sync(0xffffffffu, valid && rank < p);
+      const unsigned tb = __ballot_sync(0xffffffffu, valid && rank >= p);
+      if (valid) {
+        const int64_t dst = rank < p ? lo + nh + __popc(hb & lt) : hi - 1 - (nt + __popc(tb & lt));
+        col2[dst] = rank;
+        val2[dst] = v;
+      }
+      nh += __popc(hb);
+      nt += __popc(tb);
+    }
+  }
+}
+
 __global__ void k_gather_entries(const uint64_t* __restrict__ keys, const uint32_t* __restrict__ src,
                                  const float* __restrict__ val, int64_t nnz, uint64_t fmask,
                                  int32_t* __restrict__ col2, float* __restrict__ val2) {
@@ -500,20 +534,28 @@ cuapss_status build_side(Side& s, const PrepOptions& o, const int32_t* perm, Wor
   LAUNCH_CHECK();
   ST_TRY(ws.get(t + "rp2", (size_t)n + 1, &s.rp2));
   ST_TRY(exclusive_scan<int64_t>(newlen, s.rp2, n, s.rp2 + n, ws, t + "rp2", st));
-  // ---- remapped, row-ordered CSR via one radix sort on (new row, rank) ----
-  uint64_t* ekeys = nullptr;
-  uint32_t* evals = nullptr;
-  ST_TRY(ws.get(t + "ekeys", (size_t)nnz, &ekeys));
-  ST_TRY(ws.get(t + "evals", (size_t)nnz, &evals));
+  // ---- remapped CSR: each row's head entries (rank < p) first ----
   ST_TRY(ws.get(t + "col2", (size_t)nnz, &s.col2));
   ST_TRY(ws.get(t + "val2", (size_t)nnz, &s.val2));
-  k_entry_keys<<<grid_for(n * 32, kThreads), kThreads, 0, st>>>(s.rp0, s.col0, perm, rowinv, n,
-                                                                fbits, ekeys, evals);
-  LAUNCH_CHECK();
-  ST_TRY(radix_sort_pairs(ekeys, evals, nnz, rbits + fbits, ws, t + "ent", st));
-  k_gather_entries<<<grid_for(nnz, kThreads), kThreads, 0, st>>>(ekeys, evals, s.val0, nnz, fmask,
-                                                                 s.col2, s.val2);
-  LAUNCH_CHECK();
+  if (!o.row_sort) {
+    // rows keep their place (rp2 == rp0): split each row in one pass
+    k_split_rows<<<grid_for(n * 32, kThreads), kThreads, 0, st>>>(s.rp0, s.col0, s.val0, perm, n,
+                                                                  p, s.col2, s.val2);
+    LAUNCH_CHECK();
+  } else {
+    // rows reordered: one radix sort of all entries on (new row, rank)
+    uint64_t* ekeys = nullptr;
+    uint32_t* evals = nullptr;
+    ST_TRY(ws.get(t + "ekeys", (size_t)nnz, &ekeys));
+    ST_TRY(ws.get(t + "evals", (size_t)nnz, &evals));
+    k_entry_keys<<<grid_for(n * 32, kThreads), kThreads, 0, st>>>(s.rp0, s.col0, perm, rowinv, n,
+                                                                  fbits, ekeys, evals);
+    LAUNCH_CHECK();
+    ST_TRY(radix_sort_pairs(ekeys, evals, nnz, rbits + fbits, ws, t + "ent", st));
+    k_gather_entries<<<grid_for(nnz, kThreads), kThreads, 0, st>>>(ekeys, evals, s.val0, nnz,
+                                                                   fmask, s.col2, s.val2);
+    LAUNCH_CHECK();
+  }
   // ---- per-row statistics ----
   int64_t* tcount = nullptr;
   ST_TRY(ws.get(t + "hlen", (size_t)n, &s.hlen));

@@ -6,9 +6,10 @@
 //   rowperm   int32[n]        new row -> caller's row (rows ordered by nnz
 //                             descending, then id)
 //   rp2       int64[n+1]      CSR of the remapped, row-ordered matrix
-//   col2/val2 int32/f32[nnz]  feature ids remapped by frequency rank, sorted
-//                             ascending in each row: the head (rank < p) is a
-//                             row prefix of length hlen[r]
+//   col2/val2 int32/f32[nnz]  feature ids remapped by frequency rank; each
+//                             row holds its head entries (rank < p) first, a
+//                             prefix of length hlen[r], then its tail entries
+//                             (ascending in each part when rows are reordered)
 //   head32    f32[nb][p][128] dense head block, k-major inside a row block so
 //                             that a 32-feature slice of a block is one
 //                             contiguous 16 KB run (one bulk TMA copy)
