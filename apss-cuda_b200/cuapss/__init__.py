@@ -114,7 +114,7 @@ class RequestInfo(ctypes.Structure):
 EXPORTED = [
     "cuapss_default_opts", "cuapss_status_string", "cuapss_abi_version", "cuapss_create",
     "cuapss_destroy", "cuapss_run", "cuapss_join", "cuapss_build_index", "cuapss_feature_remap",
-    "cuapss_batch_run", "cuapss_run_shard", "cuapss_shard_blocks", "cuapss_index_create", "cuapss_index_append", "cuapss_index_query",
+    "cuapss_batch_run", "cuapss_selftest_bounded_wait", "cuapss_run_shard", "cuapss_shard_blocks", "cuapss_index_create", "cuapss_index_append", "cuapss_index_query",
     "cuapss_index_info", "cuapss_index_destroy", "cuapss_server_default_opts",
     "cuapss_server_create", "cuapss_server_submit_query", "cuapss_server_submit_append",
     "cuapss_server_wait", "cuapss_server_destroy",
@@ -152,6 +152,9 @@ def lib():
         L.cuapss_batch_run.argtypes = [_P, ctypes.POINTER(CsrDesc), ctypes.c_int32, _P, _P,
                                        ctypes.POINTER(PairsDesc), ctypes.POINTER(Stats), _P]
         L.cuapss_batch_run.restype = ctypes.c_int
+        L.cuapss_selftest_bounded_wait.argtypes = [_P, ctypes.c_int32,
+                                                   ctypes.POINTER(ctypes.c_int32)]
+        L.cuapss_selftest_bounded_wait.restype = ctypes.c_int
         L.cuapss_run_shard.argtypes = [_P, ctypes.POINTER(CsrDesc), ctypes.c_float, ctypes.c_int32,
                                        ctypes.c_int32, ctypes.POINTER(PairsDesc),
                                        ctypes.POINTER(Stats)]
@@ -276,6 +279,13 @@ class Context:
         """Self-join: (i, j, sim) numpy arrays, i < j, sorted by (i, j)."""
         d, keep = _desc(x)
         return self._pairs_call(lib().cuapss_run, (ctypes.byref(d), ctypes.c_float(t)), capacity)
+
+    def selftest_bounded_wait(self, max_polls: int = 100):
+        """(status, polls made) of the bounded-wait self-check; the expected
+        status is ETIMEOUT."""
+        polls = ctypes.c_int32()
+        s = lib().cuapss_selftest_bounded_wait(self._h, int(max_polls), ctypes.byref(polls))
+        return s, polls.value
 
     def run_shard(self, x, t: float, shard: int, nshards: int, capacity: int = 1 << 16):
         """One shard of run(): pairs whose row i lies in a 128-row block b with

@@ -49,7 +49,7 @@ typedef enum {
   CUAPSS_EINVAL = 1,    /* malformed CSR, bad option, not normalised, bad t */
   CUAPSS_ENOMEM = 2,    /* device or host allocation failed */
   CUAPSS_EOVERFLOW = 3, /* output capacity too small; count = required */
-  CUAPSS_ETIMEOUT = 4,  /* a bounded wait gave up (serving loop) */
+  CUAPSS_ETIMEOUT = 4,  /* a bounded device or host wait gave up */
   CUAPSS_ECUDA = 5,     /* a CUDA runtime call failed */
   CUAPSS_EBUSY = 6      /* admission refused: HBM budget or queue full */
 } cuapss_status;
@@ -150,6 +150,17 @@ cuapss_status cuapss_run_shard(cuapss_ctx* ctx, const cuapss_csr* x, float t,
  * there are, or -1 for bad arguments. */
 int32_t cuapss_shard_blocks(int64_t n, int32_t shard, int32_t nshards, int32_t* blocks,
                             int64_t capacity);
+
+/* Self-check of failure detection: every device wait of the tile kernels is
+ * bounded (mbarrier try-wait with a poll limit, about 2 s) and reports
+ * CUAPSS_ETIMEOUT instead of hanging. This runs a kernel that waits, with the
+ * same primitive and at most max_polls polls (1 .. 100000), on a barrier that
+ * nothing completes; it returns CUAPSS_ETIMEOUT when the wait gave up and
+ * reported it as designed (any other status is a failure), and *polls_done
+ * (may be NULL) the polls made. The context stays usable. No counterpart in
+ * the reference, whose waits are blocking host syncs. */
+cuapss_status cuapss_selftest_bounded_wait(cuapss_ctx* ctx, int32_t max_polls,
+                                           int32_t* polls_done);
 
 /* Cross-join: all pairs (a, b), a row of `a`, b row of `b`, sim >= t.
  * out->i holds the row of `a`, out->j the row of `b`; sorted by (i, j).
