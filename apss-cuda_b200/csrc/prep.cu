@@ -299,15 +299,17 @@ __device__ __forceinline__ uint32_t tail_unrot(uint32_t k, int fb) {
              : k;
 }
 
-// One warp per new row: tail entries in row order, sort keys for the
-// block-local lists (block, bucket, tag) and the half-block lists
-// (half-block, feature) and, optionally, the global lists (feature, row);
-// posting counts per tail feature.
+// One warp per new row: tail entries in row order (entry -> CSR index,
+// row in block, value, tail feature), posting counts per tail feature and,
+// when given, radix sort keys for the block-local lists (block, bucket,
+// tag), the half-block lists (half-block, feature) and the global lists
+// (feature, row).
 __global__ void k_tail_entries(const int64_t* __restrict__ rp2, const int32_t* __restrict__ col2,
                                const float* __restrict__ val2, const int32_t* __restrict__ hlen,
                                const int64_t* __restrict__ tptr, int64_t n, int p, int rbits,
                                int fb, uint32_t* __restrict__ tk, uint8_t* __restrict__ tr,
-                               float* __restrict__ tu, uint64_t* __restrict__ ckeys,
+                               float* __restrict__ tu, uint32_t* __restrict__ tf,
+                               uint64_t* __restrict__ ckeys,
                                uint32_t* __restrict__ cvals, uint64_t* __restrict__ bkeys,
                                uint32_t* __restrict__ bvals, uint64_t* __restrict__ hkeys,
                                uint32_t* __restrict__ hvals, int32_t* __restrict__ ccount) {
@@ -324,10 +326,13 @@ __global__ void k_tail_entries(const int64_t* __restrict__ rp2, const int32_t* _
       tk[t] = (uint32_t)k;
       tr[t] = (uint8_t)(r % kBlockRows);
       tu[t] = val2[k];
-      bkeys[t] = (blk << fb) | (uint64_t)tail_rot((uint32_t)f, fb);
-      bvals[t] = (uint32_t)t;
-      hkeys[t] = (hblk << fb) | (uint64_t)f;
-      hvals[t] = (uint32_t)t;
+      tf[t] = (uint32_t)f;
+      if (bkeys) {
+        bkeys[t] = (blk << fb) | (uint64_t)tail_rot((uint32_t)f, fb);
+        bvals[t] = (uint32_t)t;
+        hkeys[t] = (hblk << fb) | (uint64_t)f;
+        hvals[t] = (uint32_t)t;
+      }
       if (ckeys) {
         ckeys[t] = ((uint64_t)f << rbits) | (uint64_t)r;
         cvals[t] = (uint32_t)t;
@@ -372,6 +377,129 @@ __global__ void k_rec_fill(const uint64_t* __restrict__ keys, const uint32_t* __
     const uint32_t t = vals[k];
     const uint32_t f = (uint32_t)(keys[k] & fmask);
     rec[k] = make_uint2((f << 8) | (uint32_t)tr[t], __float_as_uint(tu[t]));
+  }
+}
+
+// ---- per-segment sorts in shared memory ----
+// The block-local lists and the half-block lists are orders of contiguous
+// row-order segments (an I block's tail entries, a half-block's) by keys
+// that are unique inside the segment (a feature occurs once per row), so the
+// sorted order is unique: one CTA sorts a segment in shared memory with a
+// bitonic network over the next power of two (padded with 0xffffffff keys)
+// and writes the postings directly. The result equals the stable global
+// radix sort by (segment, key) that is used when a segment exceeds
+// kSegMax entries.
+constexpr int kSegMax = 16384;   // entries per segment sorted in shared memory (128 KB)
+constexpr int kSegThreads = 512;
+
+__device__ __forceinline__ void seg_bitonic(uint32_t* K, uint32_t* V, int n2) {
+  for (int k = 2; k <= n2; k <<= 1) {
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      for (int i = threadIdx.x; i < (n2 >> 1); i += blockDim.x) {
+        const int lo = ((i & ~(j - 1)) << 1) | (i & (j - 1));
+        const int hi = lo + j;
+        const uint32_t a = K[lo], b = K[hi];
+        if ((a > b) == ((lo & k) == 0)) {
+          K[lo] = b;
+          K[hi] = a;
+          const uint32_t va = V[lo];
+          V[lo] = V[hi];
+          V[hi] = va;
+        }
+      }
+      __syncthreads();
+    }
+  }
+}
+
+// Loads the segment [s0, s0 + len) as (key(t), value bits) pairs, padded to
+// n2, and sorts it.
+template <typename KeyOf>
+__device__ __forceinline__ void seg_load_sort(uint32_t* K, uint32_t* V, int64_t s0, int len,
+                                              int n2, const float* __restrict__ tu, KeyOf key) {
+  for (int i = threadIdx.x; i < n2; i += blockDim.x) {
+    if (i < len) {
+      K[i] = key(s0 + i);
+      V[i] = __float_as_uint(tu[s0 + i]);
+    } else {
+      K[i] = 0xffffffffu;
+      V[i] = 0u;
+    }
+  }
+  __syncthreads();
+  seg_bitonic(K, V, n2);
+}
+
+// Shared-memory capacity (entries, a power of two >= 2) for segments of up
+// to len entries.
+inline int seg_cap(int64_t len) {
+  int c = 2;
+  while (c < len) c <<= 1;
+  return c;
+}
+
+__device__ __forceinline__ int seg_pow2(int len) {
+  int n2 = 2;
+  while (n2 < len) n2 <<= 1;
+  return n2;
+}
+
+// I-side postings of one 128-row block (one CTA per block): sort key
+// {rotated feature << 7 | row in block}; writes bil_key, bil_u, bil_len in
+// the layout of k_bil_fill.
+__global__ void __launch_bounds__(kSegThreads) k_bil_seg(const int64_t* __restrict__ bptr,
+                                                         const uint32_t* __restrict__ tf,
+                                                         const uint8_t* __restrict__ tr,
+                                                         const float* __restrict__ tu, int fb,
+                                                         uint32_t* __restrict__ bil_key,
+                                                         float* __restrict__ bil_u,
+                                                         uint8_t* __restrict__ bil_len, int cap) {
+  extern __shared__ uint32_t seg_sm[];
+  uint32_t* K = seg_sm;
+  uint32_t* V = seg_sm + cap;
+  const int64_t s0 = bptr[blockIdx.x];
+  const int len = (int)(bptr[blockIdx.x + 1] - s0);
+  if (len <= 0) return;
+  const int n2 = seg_pow2(len);
+  seg_load_sort(K, V, s0, len, n2, tu,
+                [&](int64_t t) { return (tail_rot(tf[t], fb) << 7) | (uint32_t)tr[t]; });
+  for (int i = threadIdx.x; i < len; i += blockDim.x) {
+    const uint32_t k = K[i], rf = k >> 7;
+    const uint32_t f = tail_unrot(rf, fb);
+    bil_key[s0 + i] =
+        ((f & (kTailBuckets - 1u)) << 15) | ((f >> kTailBucketBits) << 7) | (k & 127u);
+    bil_u[s0 + i] = __uint_as_float(V[i]);
+    int run = 0;
+    if (i == 0 || (K[i - 1] >> 7) != rf) {
+      int m = i + 1;
+      while (m < len && (K[m] >> 7) == rf) ++m;
+      run = m - i;
+    }
+    bil_len[s0 + i] = (uint8_t)run;
+  }
+}
+
+// J-side postings of one 64-row half-block (one CTA per half-block): sort
+// key {feature << 6 | row in half}; writes records in the layout of
+// k_rec_fill.
+__global__ void __launch_bounds__(kSegThreads) k_rec_seg(const int64_t* __restrict__ hptr,
+                                                         const uint32_t* __restrict__ tf,
+                                                         const uint8_t* __restrict__ tr,
+                                                         const float* __restrict__ tu,
+                                                         uint2* __restrict__ rec, int cap) {
+  extern __shared__ uint32_t seg_sm[];
+  uint32_t* K = seg_sm;
+  uint32_t* V = seg_sm + cap;
+  const int64_t s0 = hptr[blockIdx.x];
+  const int len = (int)(hptr[blockIdx.x + 1] - s0);
+  if (len <= 0) return;
+  const int n2 = seg_pow2(len);
+  seg_load_sort(K, V, s0, len, n2, tu,
+                [&](int64_t t) { return (tf[t] << 6) | ((uint32_t)tr[t] & 63u); });
+  const uint32_t half = (uint32_t)(blockIdx.x & 1) << 6;
+  for (int i = threadIdx.x; i < len; i += blockDim.x) {
+    const uint32_t k = K[i];
+    rec[s0 + i] = make_uint2(((k >> 6) << 8) | half | (k & 63u), V[i]);
   }
 }
 
@@ -590,9 +718,30 @@ cuapss_status build_side(Side& s, const PrepOptions& o, const int32_t* perm, Wor
                                                                       s.hlen, n, nkc, s.head16);
     LAUNCH_CHECK();
   }
-  // ---- tail: entries in row order, block-local inverted lists ----
-  CU_TRY(cudaMemcpyAsync(&s.ntail, s.tptr + n, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+  // ---- tail: segment pointers (blocks, half-blocks), host copies ----
+  const int nh = 2 * nb;  // half-blocks, the last one possibly empty
+  ST_TRY(ws.get(t + "bptr", (size_t)nb + 1, &s.bptr));
+  ST_TRY(ws.get(t + "hptr", (size_t)nh + 1, &s.hptr));
+  k_block_ptrs<<<grid_for(nb + 1, kThreads), kThreads, 0, st>>>(s.tptr, n, nb, s.bptr);
+  LAUNCH_CHECK();
+  k_half_ptrs<<<grid_for(nh + 1, kThreads), kThreads, 0, st>>>(s.tptr, n, nh, s.hptr);
+  LAUNCH_CHECK();
+  std::vector<int64_t> h_hptr((size_t)nh + 1);
+  s.h_bptr.resize(nb + 1);
+  CU_TRY(cudaMemcpyAsync(s.h_bptr.data(), s.bptr, sizeof(int64_t) * (nb + 1),
+                         cudaMemcpyDeviceToHost, st));
+  CU_TRY(cudaMemcpyAsync(h_hptr.data(), s.hptr, sizeof(int64_t) * (nh + 1),
+                         cudaMemcpyDeviceToHost, st));
   CU_TRY(cudaStreamSynchronize(st));
+  s.ntail = s.h_bptr[nb];
+  s.max_block_tail = 0;
+  for (int b = 0; b < nb; ++b)
+    s.max_block_tail = std::max<int64_t>(s.max_block_tail, s.h_bptr[b + 1] - s.h_bptr[b]);
+  int64_t max_half_tail = 0;
+  for (int h = 0; h < nh; ++h) max_half_tail = std::max<int64_t>(max_half_tail, h_hptr[h + 1] - h_hptr[h]);
+  // segments sorted in shared memory unless one exceeds kSegMax entries
+  const bool seg_sort = s.max_block_tail <= kSegMax;
+  // ---- tail: entries in row order, block-local inverted lists ----
   const int64_t T = s.ntail;
   if (T >= (int64_t)UINT32_MAX - 1) return CUAPSS_EINVAL;
   const int64_t nf = std::max<int64_t>(d - p, 0);
@@ -606,10 +755,14 @@ cuapss_status build_side(Side& s, const PrepOptions& o, const int32_t* perm, Wor
   ST_TRY(ws.get(t + "tk", (size_t)T, &s.tk));
   ST_TRY(ws.get(t + "tr", (size_t)T, &s.tr));
   ST_TRY(ws.get(t + "tu", (size_t)T, &s.tu));
-  ST_TRY(ws.get(t + "bkeys", (size_t)T, &bkeys));
-  ST_TRY(ws.get(t + "bvals", (size_t)T, &bvals));
-  ST_TRY(ws.get(t + "hkeys", (size_t)T, &hkeys));
-  ST_TRY(ws.get(t + "hvals", (size_t)T, &hvals));
+  uint32_t* tf = nullptr;
+  ST_TRY(ws.get(t + "tf", (size_t)T, &tf));
+  if (!seg_sort) {
+    ST_TRY(ws.get(t + "bkeys", (size_t)T, &bkeys));
+    ST_TRY(ws.get(t + "bvals", (size_t)T, &bvals));
+    ST_TRY(ws.get(t + "hkeys", (size_t)T, &hkeys));
+    ST_TRY(ws.get(t + "hvals", (size_t)T, &hvals));
+  }
   ST_TRY(ws.get(t + "ccount", (size_t)nf + 1, &ccount));
   if (o.want_csc) {
     ST_TRY(ws.get(t + "ckeys", (size_t)T, &ckeys));
@@ -617,34 +770,43 @@ cuapss_status build_side(Side& s, const PrepOptions& o, const int32_t* perm, Wor
   }
   CU_TRY(cudaMemsetAsync(ccount, 0, sizeof(int32_t) * (nf + 1), st));
   k_tail_entries<<<grid_for(n * 32, kThreads), kThreads, 0, st>>>(
-      s.rp2, s.col2, s.val2, s.hlen, s.tptr, n, p, rbits, fb, s.tk, s.tr, s.tu, ckeys, cvals,
-      bkeys, bvals, hkeys, hvals, ccount);
+      s.rp2, s.col2, s.val2, s.hlen, s.tptr, n, p, rbits, fb, s.tk, s.tr, s.tu, tf, ckeys,
+      cvals, bkeys, bvals, hkeys, hvals, ccount);
   LAUNCH_CHECK();
-  // block-local inverted lists: stable sort by (block, bucket, tag) keeps
-  // rows ascending inside a feature
-  ST_TRY(radix_sort_pairs(bkeys, bvals, T, bb + fb, ws, t + "bil", st));
   ST_TRY(ws.get(t + "bil_key", (size_t)T, &s.bil_key));
   ST_TRY(ws.get(t + "bil_u", (size_t)T, &s.bil_u));
   ST_TRY(ws.get(t + "bil_len", (size_t)T, &s.bil_len));
-  k_bil_fill<<<grid_for(T, kThreads), kThreads, 0, st>>>(bkeys, bvals, s.tr, s.tu, T, fb,
-                                                        s.bil_key, s.bil_u, s.bil_len);
-  LAUNCH_CHECK();
-  // J-side postings: per 64-row half-block, sorted by feature, packed
-  {
-    const int nh = 2 * nb;  // half-blocks, the last one possibly empty
+  ST_TRY(ws.get(t + "bil_rec", (size_t)T, &s.bil_rec));
+  if (seg_sort) {
+    // block-local lists in (bucket, tag, row) order and half-block records in
+    // (feature, row) order, one CTA per segment
+    if (T > 0) {
+      const int capB = seg_cap(s.max_block_tail), capH = seg_cap(max_half_tail);
+      CU_TRY(cudaFuncSetAttribute(k_bil_seg, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)(2 * sizeof(uint32_t) * capB)));
+      CU_TRY(cudaFuncSetAttribute(k_rec_seg, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)(2 * sizeof(uint32_t) * capH)));
+      k_bil_seg<<<nb, kSegThreads, 2 * sizeof(uint32_t) * capB, st>>>(
+          s.bptr, tf, s.tr, s.tu, fb, s.bil_key, s.bil_u, s.bil_len, capB);
+      LAUNCH_CHECK();
+      k_rec_seg<<<nh, kSegThreads, 2 * sizeof(uint32_t) * capH, st>>>(s.hptr, tf, s.tr, s.tu,
+                                                                     s.bil_rec, capH);
+      LAUNCH_CHECK();
+    }
+  } else {
+    // block-local inverted lists: stable sort by (block, bucket, tag) keeps
+    // rows ascending inside a feature
+    ST_TRY(radix_sort_pairs(bkeys, bvals, T, bb + fb, ws, t + "bil", st));
+    k_bil_fill<<<grid_for(T, kThreads), kThreads, 0, st>>>(bkeys, bvals, s.tr, s.tu, T, fb,
+                                                          s.bil_key, s.bil_u, s.bil_len);
+    LAUNCH_CHECK();
+    // J-side postings: per 64-row half-block, sorted by feature, packed
     ST_TRY(radix_sort_pairs(hkeys, hvals, T, std::max(1, bits_for((uint64_t)nh)) + fb, ws,
                             t + "rec", st));
-    ST_TRY(ws.get(t + "bil_rec", (size_t)T, &s.bil_rec));
-    ST_TRY(ws.get(t + "hptr", (size_t)nh + 1, &s.hptr));
     k_rec_fill<<<grid_for(T, kThreads), kThreads, 0, st>>>(hkeys, hvals, s.tr, s.tu, T,
                                                           (1ull << fb) - 1, s.bil_rec);
     LAUNCH_CHECK();
-    k_half_ptrs<<<grid_for(nh + 1, kThreads), kThreads, 0, st>>>(s.tptr, n, nh, s.hptr);
-    LAUNCH_CHECK();
   }
-  ST_TRY(ws.get(t + "bptr", (size_t)nb + 1, &s.bptr));
-  k_block_ptrs<<<grid_for(nb + 1, kThreads), kThreads, 0, st>>>(s.tptr, n, nb, s.bptr);
-  LAUNCH_CHECK();
   // ---- global inverted lists (feature, row), on request ----
   if (o.want_csc) {
     uint32_t* entpos = nullptr;
@@ -668,14 +830,8 @@ cuapss_status build_side(Side& s, const PrepOptions& o, const int32_t* perm, Wor
   LAUNCH_CHECK();
   unsigned long long hred[2] = {0, 0};
   CU_TRY(cudaMemcpyAsync(hred, red, sizeof(hred), cudaMemcpyDeviceToHost, st));
-  s.h_bptr.resize(nb + 1);
-  CU_TRY(cudaMemcpyAsync(s.h_bptr.data(), s.bptr, sizeof(int64_t) * (nb + 1),
-                         cudaMemcpyDeviceToHost, st));
   CU_TRY(cudaStreamSynchronize(st));
   s.tail_products = (int64_t)hred[0];
-  s.max_block_tail = 0;
-  for (int b = 0; b < nb; ++b)
-    s.max_block_tail = std::max<int64_t>(s.max_block_tail, s.h_bptr[b + 1] - s.h_bptr[b]);
   return CUAPSS_OK;
 }
 

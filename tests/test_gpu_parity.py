@@ -244,3 +244,34 @@ def test_row_lengths_across_sort_paths(precision):
             got = c.run(x, t)
             _check_pairs(got, oracle.apss(x, t))
             assert got[0].size > 0
+
+
+@pytest.mark.parametrize("extra", [0, 1], ids=["16384", "16385"])
+def test_block_tail_at_shared_sort_capacity(extra):
+    # Every row holds head features 0..63 (count 256, the whole head at
+    # p = 64) and 128 tail features: each 128-row block has exactly 16,384
+    # tail postings, the capacity of the per-block shared-memory sort; one
+    # extra posting in the second block sends the build to the global radix
+    # sort instead. Both must give the oracle's pairs.
+    rng = np.random.default_rng(11 + extra)
+    d = 64 + 20_000
+    rows = []
+    for r in range(256):
+        nt = 128 + (1 if (extra and r == 200) else 0)
+        f = np.concatenate([np.arange(64), 64 + rng.choice(20_000, size=nt, replace=False)])
+        rows.append(np.sort(f).astype(np.int32))
+    rp = np.zeros(len(rows) + 1, np.int64)
+    rp[1:] = np.cumsum([len(f) for f in rows])
+    col = np.concatenate(rows)
+    val = np.where(col < 64, rng.uniform(1.0, 2.0, size=len(col)),
+                   rng.uniform(0.2, 1.0, size=len(col)))
+    for r in range(256):
+        seg = slice(rp[r], rp[r + 1])
+        val[seg] /= np.linalg.norm(val[seg])
+    x = synth.Csr(rp, col, val.astype(np.float32), d)
+    for precision in (cuapss.PREC_MIXED, cuapss.PREC_FP32):
+        with cuapss.Context(precision=precision, head_width=64) as c:
+            got = c.run(x, 0.72)
+            assert c.last_stats["head_width"] == 64
+        _check_pairs(got, oracle.apss(x, 0.72))
+        assert got[0].size > 0
