@@ -391,10 +391,87 @@ __global__ void k_rec_fill(const uint64_t* __restrict__ keys, const uint32_t* __
 // kSegMax entries.
 constexpr int kSegMax = 16384;   // entries per segment sorted in shared memory (128 KB)
 constexpr int kSegThreads = 512;
+// Size classes of the segments: shared-memory capacity (entries) and threads
+// per CTA, so that small segments run many CTAs per SM.
+constexpr int kSegClasses = 3;
+constexpr int kSegCap[kSegClasses] = {1024, 4096, kSegMax};
+constexpr int kSegThr[kSegClasses] = {128, 256, kSegThreads};
 
+// One compare-exchange step of distance j < 32 on a 64-element chunk held
+// by a warp: lane l holds positions c0 + l (x0) and c0 + 32 + l (x1).
+__device__ __forceinline__ void seg_shfl_step(uint32_t& x, uint32_t& v, int pos, int j, int k) {
+  const uint32_t y = __shfl_xor_sync(0xffffffffu, x, j);
+  const uint32_t w = __shfl_xor_sync(0xffffffffu, v, j);
+  const bool up = ((pos & ~j) & k) == 0;  // direction of the pair (its lower position)
+  const bool lower = (pos & j) == 0;
+  // the lower position keeps the smaller key when ascending, the larger otherwise
+  const bool take = (lower == up) ? (y < x) : (y > x);
+  if (take) {
+    x = y;
+    v = w;
+  }
+}
+
+// Steps j = jmax .. 1 of stages k = kfirst .. klast (powers of two, each
+// stage starting at min(k / 2, jmax)) on the 64-element chunks, in
+// registers: j = 32 pairs a lane's two elements, j < 32 pairs lanes.
+__device__ __forceinline__ void seg_chunk_steps(uint32_t* K, uint32_t* V, int n2, int kfirst,
+                                                int klast, int jmax) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int c0 = warp * 64; c0 < n2; c0 += nw * 64) {
+    const int p0 = c0 + lane, p1 = p0 + 32;
+    uint32_t x0 = K[p0], x1 = K[p1], v0 = V[p0], v1 = V[p1];
+    for (int k = kfirst; k <= klast; k <<= 1) {
+      for (int j = min(k >> 1, jmax); j > 0; j >>= 1) {
+        if (j == 32) {
+          if ((x0 > x1) == ((p0 & k) == 0)) {
+            const uint32_t tx = x0, tv = v0;
+            x0 = x1;
+            v0 = v1;
+            x1 = tx;
+            v1 = tv;
+          }
+        } else {
+          seg_shfl_step(x0, v0, p0, j, k);
+          seg_shfl_step(x1, v1, p1, j, k);
+        }
+      }
+    }
+    K[p0] = x0;
+    K[p1] = x1;
+    V[p0] = v0;
+    V[p1] = v1;
+  }
+}
+
+// Bitonic sort of n2 (a power of two) key/value pairs in shared memory:
+// steps of distance >= 64 exchange through shared memory, the others run in
+// registers on 64-element chunks (one warp per chunk).
 __device__ __forceinline__ void seg_bitonic(uint32_t* K, uint32_t* V, int n2) {
-  for (int k = 2; k <= n2; k <<= 1) {
-    for (int j = k >> 1; j > 0; j >>= 1) {
+  if (n2 < 64) {
+    for (int k = 2; k <= n2; k <<= 1) {
+      for (int j = k >> 1; j > 0; j >>= 1) {
+        for (int i = threadIdx.x; i < (n2 >> 1); i += blockDim.x) {
+          const int lo = ((i & ~(j - 1)) << 1) | (i & (j - 1));
+          const int hi = lo + j;
+          const uint32_t a = K[lo], b = K[hi];
+          if ((a > b) == ((lo & k) == 0)) {
+            K[lo] = b;
+            K[hi] = a;
+            const uint32_t va = V[lo];
+            V[lo] = V[hi];
+            V[hi] = va;
+          }
+        }
+        __syncthreads();
+      }
+    }
+    return;
+  }
+  seg_chunk_steps(K, V, n2, 2, 64, 32);  // stages 2 .. 64: inside the chunks
+  __syncthreads();
+  for (int k = 128; k <= n2; k <<= 1) {
+    for (int j = k >> 1; j >= 64; j >>= 1) {
       for (int i = threadIdx.x; i < (n2 >> 1); i += blockDim.x) {
         const int lo = ((i & ~(j - 1)) << 1) | (i & (j - 1));
         const int hi = lo + j;
@@ -409,6 +486,8 @@ __device__ __forceinline__ void seg_bitonic(uint32_t* K, uint32_t* V, int n2) {
       }
       __syncthreads();
     }
+    seg_chunk_steps(K, V, n2, k, k, 32);
+    __syncthreads();
   }
 }
 
@@ -430,12 +509,27 @@ __device__ __forceinline__ void seg_load_sort(uint32_t* K, uint32_t* V, int64_t 
   seg_bitonic(K, V, n2);
 }
 
-// Shared-memory capacity (entries, a power of two >= 2) for segments of up
-// to len entries.
-inline int seg_cap(int64_t len) {
-  int c = 2;
-  while (c < len) c <<= 1;
-  return c;
+// Non-empty segments of ptr (nseg segments, host copy) grouped by size
+// class, uploaded to ids; first[c] .. first[c + 1] are class c's entries.
+inline cuapss_status seg_classes(const std::vector<int64_t>& ptr, int nseg, Workspace& ws,
+                                 const std::string& tag, cudaStream_t st, int32_t** ids,
+                                 int (&first)[kSegClasses + 1]) {
+  std::vector<int32_t> h;
+  h.reserve((size_t)nseg);
+  for (int c = 0; c < kSegClasses; ++c) {
+    first[c] = (int)h.size();
+    const int64_t lo = c == 0 ? 0 : kSegCap[c - 1];
+    for (int i = 0; i < nseg; ++i) {
+      const int64_t len = ptr[i + 1] - ptr[i];
+      if (len > lo && len <= kSegCap[c]) h.push_back(i);
+    }
+  }
+  first[kSegClasses] = (int)h.size();
+  ST_TRY(ws.get(tag, std::max<size_t>(h.size(), 1), ids));
+  if (!h.empty())
+    CU_TRY(cudaMemcpyAsync(*ids, h.data(), sizeof(int32_t) * h.size(), cudaMemcpyHostToDevice,
+                           st));
+  return CUAPSS_OK;
 }
 
 __device__ __forceinline__ int seg_pow2(int len) {
@@ -444,10 +538,11 @@ __device__ __forceinline__ int seg_pow2(int len) {
   return n2;
 }
 
-// I-side postings of one 128-row block (one CTA per block): sort key
-// {rotated feature << 7 | row in block}; writes bil_key, bil_u, bil_len in
-// the layout of k_bil_fill.
-__global__ void __launch_bounds__(kSegThreads) k_bil_seg(const int64_t* __restrict__ bptr,
+// I-side postings of one 128-row block (one CTA per block of the list
+// ids): sort key {rotated feature << 7 | row in block}; writes bil_key,
+// bil_u, bil_len in the layout of k_bil_fill.
+__global__ void __launch_bounds__(kSegThreads) k_bil_seg(const int32_t* __restrict__ ids,
+                                                         const int64_t* __restrict__ bptr,
                                                          const uint32_t* __restrict__ tf,
                                                          const uint8_t* __restrict__ tr,
                                                          const float* __restrict__ tu, int fb,
@@ -457,8 +552,9 @@ __global__ void __launch_bounds__(kSegThreads) k_bil_seg(const int64_t* __restri
   extern __shared__ uint32_t seg_sm[];
   uint32_t* K = seg_sm;
   uint32_t* V = seg_sm + cap;
-  const int64_t s0 = bptr[blockIdx.x];
-  const int len = (int)(bptr[blockIdx.x + 1] - s0);
+  const int b = ids[blockIdx.x];
+  const int64_t s0 = bptr[b];
+  const int len = (int)(bptr[b + 1] - s0);
   if (len <= 0) return;
   const int n2 = seg_pow2(len);
   seg_load_sort(K, V, s0, len, n2, tu,
@@ -479,10 +575,11 @@ __global__ void __launch_bounds__(kSegThreads) k_bil_seg(const int64_t* __restri
   }
 }
 
-// J-side postings of one 64-row half-block (one CTA per half-block): sort
-// key {feature << 6 | row in half}; writes records in the layout of
-// k_rec_fill.
-__global__ void __launch_bounds__(kSegThreads) k_rec_seg(const int64_t* __restrict__ hptr,
+// J-side postings of one 64-row half-block (one CTA per half-block of the
+// list ids): sort key {feature << 6 | row in half}; writes records in the
+// layout of k_rec_fill.
+__global__ void __launch_bounds__(kSegThreads) k_rec_seg(const int32_t* __restrict__ ids,
+                                                         const int64_t* __restrict__ hptr,
                                                          const uint32_t* __restrict__ tf,
                                                          const uint8_t* __restrict__ tr,
                                                          const float* __restrict__ tu,
@@ -490,13 +587,14 @@ __global__ void __launch_bounds__(kSegThreads) k_rec_seg(const int64_t* __restri
   extern __shared__ uint32_t seg_sm[];
   uint32_t* K = seg_sm;
   uint32_t* V = seg_sm + cap;
-  const int64_t s0 = hptr[blockIdx.x];
-  const int len = (int)(hptr[blockIdx.x + 1] - s0);
+  const int h = ids[blockIdx.x];
+  const int64_t s0 = hptr[h];
+  const int len = (int)(hptr[h + 1] - s0);
   if (len <= 0) return;
   const int n2 = seg_pow2(len);
   seg_load_sort(K, V, s0, len, n2, tu,
                 [&](int64_t t) { return (tf[t] << 6) | ((uint32_t)tr[t] & 63u); });
-  const uint32_t half = (uint32_t)(blockIdx.x & 1) << 6;
+  const uint32_t half = (uint32_t)(h & 1) << 6;
   for (int i = threadIdx.x; i < len; i += blockDim.x) {
     const uint32_t k = K[i];
     rec[s0 + i] = make_uint2(((k >> 6) << 8) | half | (k & 63u), V[i]);
@@ -737,8 +835,6 @@ cuapss_status build_side(Side& s, const PrepOptions& o, const int32_t* perm, Wor
   s.max_block_tail = 0;
   for (int b = 0; b < nb; ++b)
     s.max_block_tail = std::max<int64_t>(s.max_block_tail, s.h_bptr[b + 1] - s.h_bptr[b]);
-  int64_t max_half_tail = 0;
-  for (int h = 0; h < nh; ++h) max_half_tail = std::max<int64_t>(max_half_tail, h_hptr[h + 1] - h_hptr[h]);
   // segments sorted in shared memory unless one exceeds kSegMax entries
   const bool seg_sort = s.max_block_tail <= kSegMax;
   // ---- tail: entries in row order, block-local inverted lists ----
@@ -781,17 +877,28 @@ cuapss_status build_side(Side& s, const PrepOptions& o, const int32_t* perm, Wor
     // block-local lists in (bucket, tag, row) order and half-block records in
     // (feature, row) order, one CTA per segment
     if (T > 0) {
-      const int capB = seg_cap(s.max_block_tail), capH = seg_cap(max_half_tail);
       CU_TRY(cudaFuncSetAttribute(k_bil_seg, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)(2 * sizeof(uint32_t) * capB)));
+                                  (int)(2 * sizeof(uint32_t) * kSegMax)));
       CU_TRY(cudaFuncSetAttribute(k_rec_seg, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)(2 * sizeof(uint32_t) * capH)));
-      k_bil_seg<<<nb, kSegThreads, 2 * sizeof(uint32_t) * capB, st>>>(
-          s.bptr, tf, s.tr, s.tu, fb, s.bil_key, s.bil_u, s.bil_len, capB);
-      LAUNCH_CHECK();
-      k_rec_seg<<<nh, kSegThreads, 2 * sizeof(uint32_t) * capH, st>>>(s.hptr, tf, s.tr, s.tu,
-                                                                     s.bil_rec, capH);
-      LAUNCH_CHECK();
+                                  (int)(2 * sizeof(uint32_t) * kSegMax)));
+      int32_t *idsB = nullptr, *idsH = nullptr;
+      int fB[kSegClasses + 1], fH[kSegClasses + 1];
+      ST_TRY(seg_classes(s.h_bptr, nb, ws, t + "segB", st, &idsB, fB));
+      ST_TRY(seg_classes(h_hptr, nh, ws, t + "segH", st, &idsH, fH));
+      for (int c = 0; c < kSegClasses; ++c) {
+        const size_t sm = 2 * sizeof(uint32_t) * kSegCap[c];
+        if (fB[c + 1] > fB[c]) {
+          k_bil_seg<<<fB[c + 1] - fB[c], kSegThr[c], sm, st>>>(idsB + fB[c], s.bptr, tf, s.tr,
+                                                               s.tu, fb, s.bil_key, s.bil_u,
+                                                               s.bil_len, kSegCap[c]);
+          LAUNCH_CHECK();
+        }
+        if (fH[c + 1] > fH[c]) {
+          k_rec_seg<<<fH[c + 1] - fH[c], kSegThr[c], sm, st>>>(idsH + fH[c], s.hptr, tf, s.tr,
+                                                               s.tu, s.bil_rec, kSegCap[c]);
+          LAUNCH_CHECK();
+        }
+      }
     }
   } else {
     // block-local inverted lists: stable sort by (block, bucket, tag) keeps
