@@ -171,7 +171,6 @@ cuapss_status join_device(cuapss_ctx* ctx, const DevCsr& a, const DevCsr* b, flo
   ta.bilI_key = SA.bil_key;
   ta.bilI_len = SA.bil_len;
   ta.max_tailI = SA.max_block_tail;
-  ta.q99_tailI = SA.q99_block_tail;
   ta.bilI_u = SA.bil_u;
   ta.headJ32 = SJ->head32;
   ta.nJ = SJ->n;

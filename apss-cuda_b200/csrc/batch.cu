@@ -194,7 +194,6 @@ cuapss_status prepare_bucket(cuapss_ctx* ctx, const BatchIn& in, Bucket& b, int 
   ta.bilI_key = s.bil_key;
   ta.bilI_len = s.bil_len;
   ta.max_tailI = s.max_block_tail;
-  ta.q99_tailI = s.q99_block_tail;
   ta.bilI_u = s.bil_u;
   ta.hptrJ = s.hptr;
   ta.bilJ_rec = s.bil_rec;

@@ -836,14 +836,6 @@ cuapss_status build_side(Side& s, const PrepOptions& o, const int32_t* perm, Wor
   s.max_block_tail = 0;
   for (int b = 0; b < nb; ++b)
     s.max_block_tail = std::max<int64_t>(s.max_block_tail, s.h_bptr[b + 1] - s.h_bptr[b]);
-  s.q99_block_tail = 0;
-  if (nb > 0) {
-    std::vector<int64_t> L((size_t)nb);
-    for (int b = 0; b < nb; ++b) L[b] = s.h_bptr[b + 1] - s.h_bptr[b];
-    const int k = nb - 1 - nb / 100;  // at most nb / 100 blocks lie above L[k]
-    std::nth_element(L.begin(), L.begin() + k, L.end());
-    s.q99_block_tail = L[k];
-  }
   // segments sorted in shared memory unless one exceeds kSegMax entries
   const bool seg_sort = s.max_block_tail <= kSegMax;
   // ---- tail: entries in row order, block-local inverted lists ----

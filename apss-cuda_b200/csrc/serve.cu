@@ -488,7 +488,6 @@ cuapss_status cuapss::index_query_rows(cuapss_ctx* ctx, const cuapss_index* idx,
       ta.bilI_u = SQ.bil_u;
       ta.bilI_len = SQ.bil_len;
       ta.max_tailI = SQ.max_block_tail;
-      ta.q99_tailI = SQ.q99_block_tail;
       ta.headJ32 = G.head32;
       ta.headJ16 = G.head16;
       ta.nJ = G.n;

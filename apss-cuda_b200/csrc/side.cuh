@@ -73,7 +73,6 @@ struct Side {
   int64_t* hptr = nullptr;        // [2 nb + 1] postings of each half-block
   int64_t ntail = 0;
   int64_t max_block_tail = 0;
-  int64_t q99_block_tail = 0;     // at most 1% of the blocks hold more tail postings
   std::vector<int64_t> h_bptr;    // host copy of bptr (unit scheduling)
   int64_t tail_products = 0;      // sum over tail lists of L(L-1)/2
   double nrm_max = 1.0;           // largest row norm (FP64)

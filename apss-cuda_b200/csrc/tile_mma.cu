@@ -364,9 +364,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_tiles_mma(const TileArgs A, con
 }  // namespace
 
 // Kernel variants: more operand stages in flight when the I blocks' tails
-// fit a smaller staging area, the large staging area otherwise. The
-// 4-stage variant is kept when at most 1% of the I blocks exceed its
-// staging area (those blocks are staged in chunks).
+// fit a smaller staging area (most inputs), the large staging area otherwise.
 constexpr int kBigStages = 3, kBigCap = 11600;
 constexpr int kSmallStages = 4, kSmallCap = 6912;
 
@@ -397,7 +395,7 @@ cuapss_status launch_tiles_mma(const TileArgs& a, const void* headI16, const voi
   m.headI16 = static_cast<const uint8_t*>(headI16);
   m.headJ16 = static_cast<const uint8_t*>(headJ16);
   m.nkc = p / kKC;
-  if (a.max_tailI <= kSmallCap || a.q99_tailI <= kSmallCap)
+  if (a.max_tailI <= kSmallCap)
     k_tiles_mma<kSmallStages, kSmallCap>
         <<<grid, kThreads, Cfg<kSmallStages, kSmallCap>::kSmem, st>>>(a, m);
   else

@@ -28,7 +28,6 @@ struct TileArgs {
   const float* bilI_u;
   const uint8_t* bilI_len;  // feature run length at its first posting
   int64_t max_tailI;        // largest I-block tail (postings): picks the staging variant
-  int64_t q99_tailI;        // at most 1% of the I blocks have a longer tail
   // J side (columns of the tile)
   const float* headJ32;
   const void* headJ16;

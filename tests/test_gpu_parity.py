@@ -275,32 +275,3 @@ def test_block_tail_at_shared_sort_capacity(extra):
             assert c.last_stats["head_width"] == 64
         _check_pairs(got, oracle.apss(x, 0.72))
         assert got[0].size > 0
-
-
-def test_few_blocks_over_small_staging_area():
-    # 200 row blocks; block 0 gets 60 extra rare (tail) features per row,
-    # about 9,100 tail postings against about 2,000 in the others: the
-    # 4-stage tensor-core variant stays selected (at most 1% of the blocks
-    # exceed its staging area) and stages block 0 in two chunks.
-    x = synth.generate("plain_20k", n=25_600, seed=5)
-    rng = np.random.default_rng(5)
-    d = x.d + 100_000
-    rows, vals = [], []
-    for r in range(x.n):
-        f = x.col[x.rowptr[r]:x.rowptr[r + 1]].astype(np.int64)
-        v = x.val[x.rowptr[r]:x.rowptr[r + 1]].astype(np.float64)
-        if r < 128:
-            f = np.concatenate([f, x.d + rng.choice(100_000, size=60, replace=False)])
-            v = np.concatenate([v, rng.uniform(0.05, 0.2, size=60)])
-            o = np.argsort(f)
-            f, v = f[o], v[o] / np.linalg.norm(v)
-        rows.append(f.astype(np.int32))
-        vals.append(v.astype(np.float32))
-    rp = np.zeros(x.n + 1, np.int64)
-    rp[1:] = np.cumsum([len(f) for f in rows])
-    y = synth.Csr(rp, np.concatenate(rows), np.concatenate(vals), d)
-    with cuapss.Context(precision=cuapss.PREC_MIXED) as c:
-        got = c.run(y, 0.7)
-        assert c.last_stats["head_width"] == 1024
-    _check_pairs(got, oracle.apss(y, 0.7))
-    assert got[0].size > 0
