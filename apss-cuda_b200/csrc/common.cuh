@@ -53,12 +53,11 @@ enum : int {
 };
 
 constexpr int kBlockRows = 128;  // rows per row block (tile edge)
+// Tail staging capacity of the tile kernels: a block's feature groups are
+// staged in shared memory in chunks of at most this many groups / postings.
 // Tail postings of a row block are bucketed by the low kTailBucketBits bits
-// of the tail feature f (tail.cuh); a posting key is {bucket << kTailKeyShift
-// | tag << 7 | row in block} with tag = f >> kTailBucketBits (tail features
-// < 2^20).
-constexpr int kTailBucketBits = 13;
-constexpr int kTailKeyShift = 7 + 20 - kTailBucketBits;
+// of the tail feature (see tail.cuh).
+constexpr int kTailBucketBits = 12;
 constexpr uint32_t kTailBuckets = 1u << kTailBucketBits;
 
 inline int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }

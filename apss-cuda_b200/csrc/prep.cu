@@ -284,8 +284,8 @@ __global__ void k_head16_scatter(const int64_t* __restrict__ rp2, const int32_t*
   }
 }
 
-// Block-local lists are ordered by (bucket = f mod 2^13, tag = f >> 13):
-// the fb-bit feature rotated so that its low 13 bits lead (a bijection, so
+// Block-local lists are ordered by (bucket = f mod 2^12, tag = f >> 12):
+// the fb-bit feature rotated so that its low 12 bits lead (a bijection, so
 // equal features stay contiguous).
 __device__ __forceinline__ uint32_t tail_rot(uint32_t f, int fb) {
   return fb > kTailBucketBits
@@ -342,7 +342,7 @@ __global__ void k_tail_entries(const int64_t* __restrict__ rp2, const int32_t* _
   }
 }
 
-// I-side postings in (block, bucket, tag, row) order: key {bucket << 14 |
+// I-side postings in (block, bucket, tag, row) order: key {bucket << 15 |
 // tag << 7 | row in block}, value, and at the first posting of each
 // feature's run the run's length (a run is one feature of one block, at most
 // kBlockRows postings; 0 elsewhere).
@@ -356,8 +356,7 @@ __global__ void k_bil_fill(const uint64_t* __restrict__ keys, const uint32_t* __
     const uint64_t key = keys[k];
     const uint32_t t = vals[k];
     const uint32_t f = tail_unrot((uint32_t)(key & fmask), fb);
-    bil_key[k] =
-        ((f & (kTailBuckets - 1u)) << kTailKeyShift) | ((f >> kTailBucketBits) << 7) | (uint32_t)tr[t];
+    bil_key[k] = ((f & (kTailBuckets - 1u)) << 15) | ((f >> kTailBucketBits) << 7) | (uint32_t)tr[t];
     bil_u[k] = tu[t];
     int len = 0;
     if (k == 0 || keys[k - 1] != key) {
@@ -564,7 +563,7 @@ __global__ void __launch_bounds__(kSegThreads) k_bil_seg(const int32_t* __restri
     const uint32_t k = K[i], rf = k >> 7;
     const uint32_t f = tail_unrot(rf, fb);
     bil_key[s0 + i] =
-        ((f & (kTailBuckets - 1u)) << kTailKeyShift) | ((f >> kTailBucketBits) << 7) | (k & 127u);
+        ((f & (kTailBuckets - 1u)) << 15) | ((f >> kTailBucketBits) << 7) | (k & 127u);
     bil_u[s0 + i] = __uint_as_float(V[i]);
     int run = 0;
     if (i == 0 || (K[i - 1] >> 7) != rf) {
@@ -842,7 +841,7 @@ cuapss_status build_side(Side& s, const PrepOptions& o, const int32_t* perm, Wor
   const int64_t T = s.ntail;
   if (T >= (int64_t)UINT32_MAX - 1) return CUAPSS_EINVAL;
   const int64_t nf = std::max<int64_t>(d - p, 0);
-  // I-side keys hold a 7-bit tag above the 13-bit bucket: tail features < 2^20
+  // I-side keys hold an 8-bit tag above the 12-bit bucket: tail features < 2^20
   if (nf > (1 << 20)) return CUAPSS_EINVAL;
   const int fb = std::max(1, bits_for((uint64_t)nf));
   const int bb = std::max(1, bits_for((uint64_t)nb));

@@ -22,8 +22,8 @@
 //   bptr      int64[nb+1]     tail entries of each row block
 //   bil_key/bil_u/bil_len     block-local inverted lists: the tail postings
 //                             of each row block sorted by (bucket = f mod
-//                             2^13, tag = f >> 13, row), f = feature - p:
-//                             key {bucket << 14 | tag << 7 | row in block},
+//                             2^12, tag = f >> 12, row), f = feature - p:
+//                             key {bucket << 15 | tag << 7 | row in block},
 //                             value, and the length of each feature's run at
 //                             its first posting
 //   bil_rec   uint2[T]        the same postings per 64-row half-block, sorted by
@@ -65,7 +65,7 @@ struct Side {
   uint8_t* tr = nullptr;          // row-order tail entries: row in block, value
   float* tu = nullptr;
   int64_t* bptr = nullptr;
-  uint32_t* bil_key = nullptr;    // I-side postings {bucket << 14 | tag << 7 | row}
+  uint32_t* bil_key = nullptr;    // I-side postings {bucket << 15 | tag << 7 | row}
   float* bil_u = nullptr;
   uint8_t* bil_len = nullptr;     // run length at a feature's first posting, else 0
   uint2* bil_rec = nullptr;       // J-side postings per 64-row half-block, sorted by

@@ -4,10 +4,10 @@
 // I side (the rows of a tile; fixed for a unit of work): the block-local
 // inverted list of the 128-row block is staged in shared memory as a
 // bucketed posting list. The preprocessing sorts the block's tail postings
-// by (bucket = f mod 2^13, tag = f >> 13, row), f the tail feature, so a
+// by (bucket = f mod 2^12, tag = f >> 12, row), f the tail feature, so a
 // staged posting is {tag << 7 | row} (16 bits), its value (FP32) and, at the
 // first posting of each feature's run, the run length (8 bits); a table of
-// 8193 bucket offsets (16 bits each) delimits the buckets. Staging is a
+// 4097 bucket offsets (16 bits each) delimits the buckets. Staging is a
 // straight copy plus the offsets: no hashing, no atomics. A block with more
 // postings than the staging capacity is staged in consecutive chunks of that
 // many postings (any cut is valid: every chunk adds the products
@@ -15,8 +15,8 @@
 //
 // J side (the columns; one per tile): the tail postings of each 64-row
 // half-block sorted by feature, packed as {feature << 8 | column, value}.
-// A J posting (c, f, v) reads the two offsets of bucket f mod 2^13 and walks
-// that bucket run by run (tags ascend) to the run with tag f >> 13; each of
+// A J posting (c, f, v) reads the two offsets of bucket f mod 2^12 and walks
+// that bucket run by run (tags ascend) to the run with tag f >> 12; each of
 // its postings (r, u) adds u * v into the shared-memory accumulator
 // acc[r][c] with an integer atomic on a fixed-point grid of 2^-30: FP32
 // products are rounded to the grid and the integer sums are exact in any
@@ -34,8 +34,8 @@
 
 namespace cuapss {
 
-constexpr int kStagePostings = 11600;  // default postings per staged chunk (16-bit offsets)
-constexpr uint32_t kMaxTailFeature = (1u << 20) - 1;  // 7-bit tag above 13-bit bucket
+constexpr int kStagePostings = 12800;  // default postings per staged chunk (16-bit offsets)
+constexpr uint32_t kMaxTailFeature = (1u << 20) - 1;  // 8-bit tag above 12-bit bucket
 constexpr float kTailScale = 1073741824.0f;              // 2^30
 constexpr float kTailUnscale = 9.313225746154785e-10f;   // 2^-30
 
@@ -106,7 +106,7 @@ __device__ __forceinline__ TailI stage_tail_chunk(const TileArgs& A, const TailS
   }
   for (int e = ltid; e < P; e += NT) {
     const uint32_t key = __ldg(&A.bilI_key[e0 + e]);
-    S.et[e] = (uint16_t)(key & ((1u << kTailKeyShift) - 1u));
+    S.et[e] = (uint16_t)(key & 0x7fffu);
     S.eu[e] = __ldg(&A.bilI_u[e0 + e]);
     int len = __ldg(&A.bilI_len[e0 + e]);
     if (e == 0 && len == 0) {
@@ -117,8 +117,8 @@ __device__ __forceinline__ TailI stage_tail_chunk(const TileArgs& A, const TailS
     }
     S.en[e] = (uint8_t)(len < P - e ? len : P - e);
     // offsets: this posting starts every bucket after its predecessor's
-    const int bk = (int)(key >> kTailKeyShift);
-    const int bp = e > 0 ? (int)(__ldg(&A.bilI_key[e0 + e - 1]) >> kTailKeyShift) : -1;
+    const int bk = (int)(key >> 15);
+    const int bp = e > 0 ? (int)(__ldg(&A.bilI_key[e0 + e - 1]) >> 15) : -1;
     for (int b = bp + 1; b <= bk; ++b) S.boff[b] = (uint16_t)e;
     if (e == P - 1)
       for (int b = bk + 1; b <= (int)kTailBuckets; ++b) S.boff[b] = (uint16_t)P;

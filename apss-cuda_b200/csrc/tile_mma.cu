@@ -365,8 +365,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_tiles_mma(const TileArgs A, con
 
 // Kernel variants: more operand stages in flight when the I blocks' tails
 // fit a smaller staging area (most inputs), the large staging area otherwise.
-constexpr int kBigStages = 3, kBigCap = 11600;
-constexpr int kSmallStages = 4, kSmallCap = 6912;
+constexpr int kBigStages = 3, kBigCap = 12768;
+constexpr int kSmallStages = 4, kSmallCap = 7936;
 
 // Opts the kernels into their dynamic shared memory once per device (outside
 // any stream capture when called ahead of it).

@@ -24,7 +24,7 @@ struct TileArgs {
   const int32_t* blkmaxI;
   const float* hnormI;
   const int64_t* bptrI;     // tail postings of each I block
-  const uint32_t* bilI_key; // {bucket << 14 | tag << 7 | row}, (bucket, tag, row) order
+  const uint32_t* bilI_key; // {bucket << 15 | tag << 7 | row}, (bucket, tag, row) order
   const float* bilI_u;
   const uint8_t* bilI_len;  // feature run length at its first posting
   int64_t max_tailI;        // largest I-block tail (postings): picks the staging variant
