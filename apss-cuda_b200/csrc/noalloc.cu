@@ -15,14 +15,18 @@
 // CUAPSS_EINVAL. The array exists on every device this library's module is
 // loaded on, until the process exits. Host code never hands the array's name
 // to a kernel (in host code that name is a host-side shadow, not a device
-// address): the first call made on a device, with that device current, looks
-// up the device address with cudaGetSymbolAddress (return code checked) and
-// keeps it; later calls reuse it. That first call can load the module, so it
-// should come before any stream capture. The array keeps the last call's
-// contents; each call clears what must start at zero (the error flag and the
-// caller's counts array). Calls whose GPU work overlaps (two streams, two
-// host threads, two contexts on one device) share the array and race:
-// serialise them.
+// address): every call, with its device current, looks up the device address
+// with cudaGetSymbolAddress (return code checked), so a reset device or a
+// recreated primary context never leaves a stale address behind. The first
+// call on a device can load the module, so it should come before any stream
+// capture. Every call waits for its own work before it returns (it reads an
+// error flag back), so the host is blocked until the remap is done. The array
+// keeps the last call's contents; each call clears what must start at zero
+// (the error flag and the caller's counts array). Calls whose GPU work
+// overlaps (two streams, two host threads, two contexts on one device) share
+// the array and race: serialise them. When a call returns CUAPSS_EINVAL after
+// its launches (a bad column id or an unsorted row), perm and counts hold
+// partial results and must not be used.
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -50,10 +54,6 @@ constexpr size_t kOffFlags = kOffParts + 256 * ((4 * kNoAllocScanParts + 255) / 
 constexpr size_t kNoAllocScratchBytes = kOffFlags + 256;  // about 1.6 MB
 
 static __device__ __align__(256) unsigned char g_remap_scratch[kNoAllocScratchBytes];
-
-constexpr int kMaxDevices = 64;
-std::mutex g_setup_mu;
-void* g_scratch_ptr[kMaxDevices] = {};
 
 constexpr int kThreads = 256;
 
@@ -107,20 +107,17 @@ inline unsigned grid_for(int64_t work) {
   return (unsigned)(g < 148 * 8 ? g : 148 * 8);
 }
 
-// Device address of the scratch array on the current device (set up once).
+// Device address of the scratch array on the current device, looked up on
+// every call (cheap once the module is loaded).
 cuapss_status scratch_for(int dev, unsigned char** out) {
-  if (dev < 0 || dev >= kMaxDevices) return CUAPSS_EINVAL;
-  std::lock_guard<std::mutex> lk(g_setup_mu);
-  if (!g_scratch_ptr[dev]) {
-    void* p = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&p, g_remap_scratch);
-    if (e != cudaSuccess || !p) {
-      record_cuda_error(e, "cudaGetSymbolAddress(g_remap_scratch)", __FILE__, __LINE__);
-      return CUAPSS_ECUDA;
-    }
-    g_scratch_ptr[dev] = p;
+  if (dev < 0) return CUAPSS_EINVAL;
+  void* p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_remap_scratch);
+  if (e != cudaSuccess || !p) {
+    record_cuda_error(e, "cudaGetSymbolAddress(g_remap_scratch)", __FILE__, __LINE__);
+    return CUAPSS_ECUDA;
   }
-  *out = static_cast<unsigned char*>(g_scratch_ptr[dev]);
+  *out = static_cast<unsigned char*>(p);
   return CUAPSS_OK;
 }
 

@@ -5,11 +5,15 @@
 
 namespace cuapss {
 
-// A waiting thread sleeps in mbarrier.try_wait for up to kSuspendNs per poll
-// (it is woken as soon as the phase completes); after kMaxPolls polls (about
-// 2 s) the wait gives up and the kernel reports kErrTimeout.
+// Bounded waits. A waiting thread sleeps in mbarrier.try_wait for up to
+// kSuspendNs per poll (it is woken as soon as the phase completes) and gives
+// up once kWaitLimitNs of device time (%globaltimer) have passed since its
+// first unsuccessful poll; the kernel then reports kErrTimeout. kMaxPolls is
+// a second bound on the poll count (each poll takes well over 100 ns, so it
+// lies far beyond the time limit) in case the timer stood still.
 constexpr uint32_t kSuspendNs = 20000;
-constexpr uint32_t kMaxPolls = 100000;
+constexpr uint64_t kWaitLimitNs = 2000000000ull;  // 2 s
+constexpr uint32_t kMaxPolls = 1u << 30;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return (uint32_t)__cvta_generic_to_shared(p);
@@ -50,10 +54,22 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
   return ok != 0;
 }
 
-// Bounded wait for the phase with the given parity; false on give-up.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
-  for (uint32_t i = 0; i < kMaxPolls; ++i)
+__device__ __forceinline__ uint64_t globaltimer_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Bounded wait for the phase with the given parity: true once it completed,
+// false after limit_ns of device time.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity,
+                                          uint64_t limit_ns = kWaitLimitNs) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const uint64_t t0 = globaltimer_ns();
+  for (uint32_t i = 0; i < kMaxPolls; ++i) {
     if (mbar_try_wait(bar, parity)) return true;
+    if (globaltimer_ns() - t0 >= limit_ns) return false;
+  }
   return false;
 }
 

@@ -138,7 +138,13 @@ __global__ void __launch_bounds__(kThreads, 1) k_tiles_fp32(const TileArgs A) {
           const bool ok = mbar_wait(&S.bar[stage], parity[stage]);
           parity[stage] ^= 1u;
           if (__syncthreads_or(!ok)) {
-            if (tid == 0) atomicOr(A.err, kErrTimeout);
+            if (tid == 0) {
+              atomicOr(A.err, kErrTimeout);
+              // the next slice's copy is in flight into the other stage: let
+              // it land (bounded) before the CTA's shared memory goes away
+              if (kc + 1 < nchunks) mbar_wait(&S.bar[stage ^ 1], parity[stage ^ 1]);
+            }
+            __syncthreads();
             return;
           }
           const float4* a4 = reinterpret_cast<const float4*>(S.a[stage]);

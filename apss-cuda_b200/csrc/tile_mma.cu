@@ -104,12 +104,15 @@ __device__ __forceinline__ SmemM carve(uint8_t* raw) {
   return s;
 }
 
-// Bounded wait that also gives up when another role raised the abort flag.
+// Bounded wait (kWaitLimitNs of device time) that also gives up when another
+// role raised the abort flag.
 __device__ __forceinline__ bool wait_or_abort(uint64_t* bar, uint32_t parity,
                                               const volatile int* abort) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const uint64_t t0 = globaltimer_ns();
   for (uint32_t i = 0; i < kMaxPolls; ++i) {
     if (mbar_try_wait(bar, parity)) return true;
-    if (*abort) return false;
+    if (*abort || globaltimer_ns() - t0 >= kWaitLimitNs) return false;
   }
   return false;
 }
@@ -185,7 +188,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_tiles_mma(const TileArgs A, con
       // drain: the last copies issued must have landed before the CTA exits
       const uint32_t first = it > (uint32_t)STAGES ? it - STAGES : 0u;
       for (uint32_t q = first; q < it; ++q)
-        mbar_wait(&S.full[q % STAGES], (q / STAGES) & 1u);
+        if (!mbar_wait(&S.full[q % STAGES], (q / STAGES) & 1u)) raise_abort(A, abort);
     }
     __syncwarp();
   } else if (warp == 1) {
@@ -228,7 +231,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_tiles_mma(const TileArgs A, con
       // drain: every MMA issued must be complete before tensor memory is freed
       if (it > 0) {
         umma_commit(S.drain);
-        mbar_wait(S.drain, 0);
+        if (!mbar_wait(S.drain, 0)) raise_abort(A, abort);
       }
     }
     __syncwarp();

@@ -153,7 +153,7 @@ def lib():
                                        ctypes.POINTER(PairsDesc), ctypes.POINTER(Stats), _P]
         L.cuapss_batch_run.restype = ctypes.c_int
         L.cuapss_selftest_bounded_wait.argtypes = [_P, ctypes.c_int32,
-                                                   ctypes.POINTER(ctypes.c_int32)]
+                                                   ctypes.POINTER(ctypes.c_int64)]
         L.cuapss_selftest_bounded_wait.restype = ctypes.c_int
         L.cuapss_run_shard.argtypes = [_P, ctypes.POINTER(CsrDesc), ctypes.c_float, ctypes.c_int32,
                                        ctypes.c_int32, ctypes.POINTER(PairsDesc),
@@ -280,12 +280,12 @@ class Context:
         d, keep = _desc(x)
         return self._pairs_call(lib().cuapss_run, (ctypes.byref(d), ctypes.c_float(t)), capacity)
 
-    def selftest_bounded_wait(self, max_polls: int = 100):
-        """(status, polls made) of the bounded-wait self-check; the expected
-        status is ETIMEOUT."""
-        polls = ctypes.c_int32()
-        s = lib().cuapss_selftest_bounded_wait(self._h, int(max_polls), ctypes.byref(polls))
-        return s, polls.value
+    def selftest_bounded_wait(self, limit_us: int = 1000):
+        """(status, device ns waited) of the bounded-wait self-check with a
+        deadline of limit_us; the expected status is ETIMEOUT."""
+        waited = ctypes.c_int64()
+        s = lib().cuapss_selftest_bounded_wait(self._h, int(limit_us), ctypes.byref(waited))
+        return s, waited.value
 
     def run_shard(self, x, t: float, shard: int, nshards: int, capacity: int = 1 << 16):
         """One shard of run(): pairs whose row i lies in a 128-row block b with

@@ -81,12 +81,24 @@ CONFIGS = {
 
 
 _lib = None
+_lib_path = os.path.join(_LIB_DIR, "libcuapss_synth.so")
+
+
+def use_library(path: str) -> None:
+    """Generate with another build of the same generator source (the CPU
+    reference arm of the benchmark uses the copy built under oracle/lib/ so
+    that it maps no library of the package). Call before the first
+    generate()."""
+    global _lib_path
+    if _lib is not None and path != _lib_path:
+        raise RuntimeError("the generator library is already loaded")
+    _lib_path = path
 
 
 def lib():
     global _lib
     if _lib is None:
-        path = os.path.join(_LIB_DIR, "libcuapss_synth.so")
+        path = _lib_path
         if not os.path.exists(path):
             raise RuntimeError(f"{path} is not built; run __graft_entry__.build()")
         L = ctypes.CDLL(path)

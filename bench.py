@@ -1,31 +1,42 @@
 #!/usr/bin/env python3
 """All-pairs cosine similarity search benchmark (pairs/s).
 
-Workload (default): the hybrid APSS at scale -- n = 800,000 vectors,
-d = 50,000, nnz/row lognormal(mean 75, sigma 1.0) clipped at 3,000, Zipf(1.1)
-feature ids, tf-log values, 2% planted near-duplicates, threshold t = 0.7,
-seeded synthetic data (the reference's corpus is not distributed).
+Workload (default, `mixed_1m`): n = 1,000,000 vectors, d = 1,000,000,
+nnz/row lognormal(mean 120, sigma 1.0) clipped at 5,000, Zipf(1.2) feature
+ids, tf-log values, 2% planted near-duplicates, threshold t = 0.7, seeded
+synthetic data (the reference's corpus is not distributed).
 
 The headline is the mixed-precision path (BF16 head on tcgen05 tensor
-cores, FP32 tail, FP64 rescore of the error band -- exact pair set); the
-plain FP32 hybrid is timed on the same data and reported beside it.
+cores, FP32 tail, FP64 rescore of the error band -- exact pair set). Beside
+it, on the same data and outside the headline's timed region:
+  * oracle_check: the FP64 oracle on sampled query rows; the emitted pairs
+    that touch them must be the oracle's set, with the largest |sim - FP64|;
+  * t_sweep: the same self-join at the workload's other thresholds, each
+    with its own oracle check;
+  * named_head: the dense-head width the workload names (4,096 features),
+    when it differs from the library's choice;
+  * plain_fp32: the plain FP32 hybrid, mixed_over_plain = its time / ours;
+  * cpu_baseline: the OpenMP FP32 hybrid on the host cores, on a bounded
+    sample of query rows, extrapolated to the whole self-join.
 
-A step is one complete self-join of that matrix: validate, frequency remap,
-row order, head block and inverted lists, all 128 x 128 pair tiles, the exact
-finalize and the sorted (i, j, sim) list. value = n(n-1)/2 pairs per step x
-steps x ranks / device time (inputs already in HBM). e2e is the same metric
-through the C ABI with pinned host buffers: the CSR upload and the pair-list
-download are inside the timed region.
+A step is one complete self-join: validate, frequency remap, head block and
+inverted lists, all 128 x 128 pair tiles, the exact finalize and the sorted
+(i, j, sim) list. value = n(n-1)/2 pairs / device time per step (inputs
+already in HBM). e2e is the same metric through the C ABI with pinned host
+buffers: the CSR upload and the pair-list download are inside the timed
+region.
 
   python bench.py [--gpus N --steps K --warmup W] [--impl reference]
-  python bench.py --workload mixed_1m   # n = d = 1,000,000, Zipf(1.2), mean nnz 120
+  python bench.py --workload plain_800k # n = 800k, d = 50k, t sweep 0.5 / 0.7 / 0.9
   python bench.py --workload batch      # 4,096 uneven instances, per-instance t
   python bench.py --workload serve      # 5M resident index, request server, p50/p99
-Multi-GPU (torchrun): the default workload's self-join is split into row-block
-shards (rank r takes the 128-row blocks b with b % N == r, cuapss_run_shard);
-there is no cross-GPU exchange; value = the job's pairs / the slowest rank's
-time (total work fixed: strong scaling). The batch and serve workloads run
-one replica per rank.
+Multi-GPU: `--gpus N` starts N ranks (torch.distributed.run) unless it runs
+under a launcher already. The self-join is split into row-block shards
+(rank r takes the 128-row blocks b with b % N == r, cuapss_run_shard); there
+is no cross-GPU exchange on the data path; value = the job's n(n-1)/2 pairs
+/ the slowest rank's device time (total work fixed: strong scaling). The
+batch and serve workloads run one replica per rank. `--dry-shards` runs the
+rank layout on CPU (gloo) and checks that the shards partition the blocks.
 """
 from __future__ import annotations
 
@@ -33,6 +44,7 @@ import argparse
 import ctypes
 import json
 import os
+import socket
 import subprocess
 import sys
 import tempfile
@@ -43,17 +55,27 @@ for _p in (ROOT, os.path.join(ROOT, "apss-cuda_b200")):
     if _p not in sys.path:
         sys.path.insert(0, _p)
 
-METRIC = "APSS pairs/s (all-pairs throughput n(n-1)/2 / time, exact pair set vs FP64 oracle)"
-WORKLOAD = "plain_800k"
+METRIC = "APSS pairs/s, mixed-prec vs plain FP32, exact pair set; query p50/p99 ms"
+WORKLOAD = "mixed_1m"
+# thresholds of each self-join workload (the headline t is --t)
+T_SWEEP = {"mixed_1m": (0.5, 0.7, 0.8), "plain_800k": (0.5, 0.7, 0.9), "plain_20k": (0.9,)}
+# dense-head width a workload names, timed beside the library's own choice
+NAMED_HEAD = {"mixed_1m": 4096}
+# the reference's own CPU search handles feature ids below this (main.cu:17)
+REF_MAX_DIMS = 198456
+SIM_TOL = 1e-6
 
 
 def peaks():
+    """(HBM GB/s, BF16 TFLOP/s burst, BF16 TFLOP/s sustained, source)."""
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
             m = json.load(f)
-        return float(m["hbm_gbs"]), float(m["bf16_tflops"]), "measured"
+        bf = float(m["bf16_tflops"])
+        return (float(m["hbm_gbs"]), bf, float(m.get("bf16_tflops_sustained", bf)),
+                "measured")
     except Exception:
-        return 6650.0, 1590.0, "fallback"
+        return 6650.0, 1590.0, 1400.0, "fallback"
 
 
 class Clocks:
@@ -107,105 +129,451 @@ class Clocks:
                 "reasons": reasons, "samples": len(rows)}
 
 
-def cpu_baseline(x, t, p, budget_s=12.0):
-    """OpenMP FP32 hybrid (oracle/oracle.c cpu_hybrid_apss) on a bounded
-    sample of query rows of the same workload; extrapolated to the full job."""
+def sample_rows(n: int, k: int, seed: int):
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    return np.sort(rng.choice(n, size=min(n, k), replace=False)).astype(np.int64)
+
+
+def cpu_sample(x, t, p, budget_s, seed=1, threads=0, hybrid=None):
+    """OpenMP FP32 hybrid (oracle/oracle.c) on random query rows of the same
+    workload, grown until about budget_s of query time; extrapolated to the
+    whole self-join: value = n(n-1)/2 / (prep + query time x all pairs /
+    covered pairs). Returns (dict, hybrid handle)."""
+    import numpy as np
     from oracle import oracle
-    threads = oracle.max_threads()
-    q = 32
-    _, prep, qs = oracle.cpu_hybrid(x, t, p, 0, q, threads)
-    per_row = max(qs / q, 1e-6)
-    q = int(min(x.n, max(q, budget_s / per_row)))
-    _, prep, qs = oracle.cpu_hybrid(x, t, p, 0, q, threads)
-    covered = q * (x.n - 1) - q * (q - 1) / 2
+    threads = threads or oracle.max_threads()
+    h = hybrid or oracle.CpuHybrid(x, p, threads)
+    q = 64
+    while True:
+        rows = sample_rows(x.n, q, seed)
+        _, qs = h.query(t, rows)
+        if qs >= budget_s or q >= x.n:
+            break
+        q = int(min(x.n, max(2 * q, q * 1.2 * budget_s / max(qs, 1e-3))))
+    covered = float(np.sum(x.n - 1 - rows))
     total = x.n * (x.n - 1) / 2
-    full_time = prep + qs * total / covered
-    return {"value": total / full_time, "unit": "pairs/s", "cores": threads, "kind": "port",
-            "sample": f"query rows 0..{q} of the workload against all j > i "
-                      f"({covered:.3g} of {total:.3g} pairs, {qs:.1f} s) + full preprocessing "
-                      f"({prep:.1f} s), extrapolated to the whole self-join"}
+    full_s = h.prep_s + qs * total / max(covered, 1.0)
+    return ({"value": total / full_s, "unit": "pairs/s", "cores": threads, "kind": "port",
+             "sample": f"{len(rows)} random query rows against all j > i ({covered:.3g} of "
+                       f"{total:.3g} pairs, {qs:.1f} s) after the full preprocessing "
+                       f"({h.prep_s:.1f} s, p = {p}), extrapolated to the whole self-join",
+             "sample_s": qs}, h)
+
+
+def repo_libraries():
+    """Shared libraries of this repository mapped into this process."""
+    found = set()
+    try:
+        with open("/proc/self/maps") as f:
+            for ln in f:
+                path = ln.split()[-1] if len(ln.split()) >= 6 else ""
+                if path.startswith(ROOT) and ".so" in path:
+                    found.add(os.path.relpath(path, ROOT))
+    except OSError:
+        pass
+    return sorted(found)
 
 
 def run_reference(args, rank, world):
-    """--impl reference: the reference's own CPU search (InvertedIndex_search,
-    main.cu:104-141, built from its source into oracle/_ref/) on bounded
-    samples of the workload, one process per host core group."""
+    """--impl reference: the CPU implementation of the path on the host cores.
+
+    The reference's CPU search (InvertedIndex_search, main.cu:104-141) sizes
+    its lists to max_dims = 198,456 feature ids (main.cu:17) and hard-codes
+    t = 0.8 (main.cu:133), so on this workload (d = 1,000,000, t = 0.7) it
+    cannot run; its algorithm runs as the oracle's OpenMP restatement of the
+    same hybrid (kind "port"), with every host thread. Inputs come from the
+    generator built under oracle/lib/, so no library of the package is
+    mapped. Each step is a bounded sample of query rows; rank 0 alone runs."""
     if rank != 0:
         return
     from cuapss import synth
     from oracle import oracle
-    exe = oracle.ref_cpu_search_path()
-    x = synth.generate(WORKLOAD, n=args.n) if args.n else synth.generate(WORKLOAD)
-    total_pairs = x.n * (x.n - 1) / 2
-    if exe is None:
-        # no reference build here: time the CPU port instead
-        vals = []
-        for _ in range(args.warmup + args.steps):
-            vals.append(cpu_baseline(x, args.t, 64, budget_s=8.0))
-        v = vals[-args.steps:]
-        value = sum(b["value"] for b in v) / len(v)
-        line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "pairs/s",
-                "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-                "higher_is_better": True, "config": {"workload": WORKLOAD, "n": x.n, "t": args.t},
-                "cpu_baseline": dict(v[-1], value=value),
-                "e2e": {"value": value, "unit": "pairs/s", "h2d_bytes_per_step": 0,
-                        "d2h_bytes_per_step": 0}}
-        print(json.dumps(line))
-        return
-    nproc = max(1, min(os.cpu_count() or 1, 32))
-    n_e = min(x.n, args.ref_index_rows)
-    e = x.rows(0, n_e)
-    td = tempfile.mkdtemp()
-    pe = os.path.join(td, "e.csr")
-    e.save(pe)
-
-    def one_step(q_per_proc):
-        procs, files = [], []
-        for k in range(nproc):
-            lo = n_e + k * q_per_proc
-            if lo + q_per_proc > x.n:
-                lo = (k * q_per_proc) % max(1, x.n - q_per_proc)
-            b = x.rows(lo, lo + q_per_proc)
-            pb = os.path.join(td, f"b{k}.csr")
-            b.save(pb)
-            files.append(pb)
-            procs.append(subprocess.Popen([exe, pb, pe], stdout=subprocess.PIPE,
-                                          stderr=subprocess.DEVNULL, text=True))
-        secs = []
-        for pr in procs:
-            out, _ = pr.communicate()
-            for ln in out.splitlines():
-                if ln.startswith("search_seconds="):
-                    secs.append(float(ln.split("=")[1]))
-        if len(secs) != nproc:
-            raise RuntimeError("reference harness failed")
-        return max(secs)
-
-    # calibrate: seconds per query row
-    t1 = one_step(2)
-    q = max(2, int(args.ref_step_s / max(t1 / 2, 1e-3)))
-    for _ in range(args.warmup):
-        one_step(q)
-    times = [one_step(q) for _ in range(args.steps)]
-    secs = sum(times) / len(times)
-    ordered = nproc * q * n_e
-    value = 0.5 * ordered / secs  # unordered-pair rate of a self-join by this method
-    sample = (f"{nproc} processes x {q} query rows against the reference's inverted index of "
-              f"{n_e} rows ({ordered:.3g} ordered pairs per step, {secs:.1f} s); a self-join "
-              f"visits each unordered pair twice, so value = ordered rate / 2")
+    synth.use_library(os.path.join(ROOT, "oracle", "lib", "libworkload.so"))
+    if not os.path.exists(os.path.join(ROOT, "oracle", "lib", "libworkload.so")):
+        oracle.build()
+    x = synth.generate(args.workload, n=args.n) if args.n else synth.generate(args.workload)
+    threads = oracle.max_threads()
+    h = None
+    vals, samples = [], []
+    for k in range(args.warmup + args.steps):
+        r, h = cpu_sample(x, args.t, 128, args.ref_step_s, seed=100 + k, threads=threads,
+                          hybrid=h)
+        if k >= args.warmup:
+            vals.append(r["value"])
+            samples.append(r)
+    value = sum(vals) / len(vals)
+    qs = sum(s["sample_s"] for s in samples) / len(samples)
+    why = (f"d = {x.d} exceeds the reference CPU search's max_dims = {REF_MAX_DIMS} "
+           f"(main.cu:17) and its t is fixed at 0.8 (main.cu:133): the same hybrid runs as "
+           f"the oracle's OpenMP port") if x.d > REF_MAX_DIMS or args.t != 0.8 else None
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "pairs/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": secs * 1e3, "higher_is_better": True, "scaling": "weak",
+            "ms_per_step": qs * 1e3, "higher_is_better": True, "scaling": "strong",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "n": x.n, "d": x.d, "t": 0.8,
-                       "note": "the reference's CPU search has t = 0.8 hard-coded"},
-            "cpu_baseline": {"value": value, "unit": "pairs/s", "cores": nproc,
-                             "kind": "reference", "sample": sample},
+            "config": {"workload": args.workload, "n": x.n, "d": x.d, "nnz": x.nnz,
+                       "t": args.t},
+            "cpu_baseline": {"value": value, "unit": "pairs/s", "cores": threads,
+                             "kind": "port", "sample": samples[-1]["sample"]},
             "e2e": {"value": value, "unit": "pairs/s", "h2d_bytes_per_step": 0,
-                    "d2h_bytes_per_step": 0}}
+                    "d2h_bytes_per_step": 0},
+            "note": why, "mapped_repo_libraries": repo_libraries()}
+    h.close()
     print(json.dumps(line))
 
 
+def oracle_pairs_check(x, got, rows, want, t):
+    """Pairs of `got` (i, j, sim) that touch `rows` against the FP64 oracle's
+    pairs of those rows at threshold t (want = the oracle at a lower or equal
+    threshold, filtered here)."""
+    import numpy as np
+    gi, gj, gs = got
+    wi, wj, ws = want
+    keep = ws >= t
+    wi, wj, ws = wi[keep], wj[keep], ws[keep]
+    equal = len(gi) == len(wi) and bool(np.array_equal(gi, wi) and np.array_equal(gj, wj))
+    err = float(np.max(np.abs(gs.astype(np.float64) - ws))) if equal and len(ws) else (
+        0.0 if equal else None)
+    return {"rows": int(len(rows)), "pairs": int(len(wi)), "pairs_found": int(len(gi)),
+            "pairs_equal": equal, "max_abs_err": err}
+
+
+class Runner:
+    """A context and device output buffers that grow on EOVERFLOW."""
+
+    def __init__(self, cuapss, torch, dev, local, stream, **opts):
+        self.cuapss, self.torch, self.dev = cuapss, torch, dev
+        self.ctx = cuapss.Context(device=local, stream=stream.cuda_stream, **opts)
+        self.cap = 1 << 22
+        self.out = self._alloc(self.cap)
+        self.npairs = 0
+
+    def _alloc(self, c):
+        t = self.torch
+        return {"i": t.empty(c, dtype=t.int32, device="cuda"),
+                "j": t.empty(c, dtype=t.int32, device="cuda"),
+                "sim": t.empty(c, dtype=t.float32, device="cuda")}
+
+    def step(self, t, shard=0, nshards=1):
+        while True:
+            try:
+                if nshards > 1:
+                    self.npairs = self.ctx.run_shard_device(self.dev, t, shard, nshards, self.out)
+                else:
+                    self.npairs = self.ctx.run_device(self.dev, t, self.out)
+                return self.npairs
+            except self.cuapss.CuapssError as e:
+                if e.status != self.cuapss.EOVERFLOW:
+                    raise
+                self.cap = self.ctx.required + 1024
+                self.out = None
+                self.out = self._alloc(self.cap)
+
+    def pairs(self):
+        m = self.npairs
+        return self.out["i"][:m], self.out["j"][:m], self.out["sim"][:m]
+
+    def close(self):
+        self.ctx.close()
+        self.out = None
+
+
+def timed(runner, torch, stream, t, steps, warmup, clocks=None, shard=0, nshards=1):
+    """warmup untimed steps, then `steps` steps between CUDA events on the
+    library's stream; returns (ms per step, per-step stats)."""
+    for _ in range(max(warmup, 0)):
+        runner.step(t, shard, nshards)
+    torch.cuda.synchronize()
+    stats = []
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    if clocks:
+        clocks.__enter__()
+    e0.record(stream)
+    for _ in range(steps):
+        runner.step(t, shard, nshards)
+        stats.append(dict(runner.ctx.last_stats))
+    e1.record(stream)
+    torch.cuda.synchronize()
+    if clocks:
+        clocks.__exit__()
+    return e0.elapsed_time(e1) / steps, stats
+
+
+def mean_stage(stats):
+    return {k: sum(s[k] for s in stats) / len(stats)
+            for k in ("ms_preprocess", "ms_tiles", "ms_finalize", "ms_total")}
+
+
+def tile_roofline(stats, p, pairs, n, world, prec_mixed, x, peaks_):
+    """Roofline of the pair-tile kernel from its CUDA-event time."""
+    hbm, bf16, bf16_sus, src = peaks_
+    import cuapss
+    tile_ms = sum(s["ms_tiles"] for s in stats) / len(stats)
+    s0 = stats[-1]
+    head_flops = 2.0 * p * pairs
+    nb = (n + 127) // 128
+    if world > 1:
+        head_flops *= s0["tiles"] / (nb * (nb + 1) / 2)
+    if prec_mixed:
+        achieved = head_flops / (tile_ms / 1e3) / 1e12
+        tr = TILE_TRAFFIC_PER_TILE.get(p)
+        return {"bound": "tensor", "achieved": achieved, "peak": bf16_sus, "unit": "TFLOP/s",
+                "frac": achieved / bf16_sus,
+                "traffic": tr * s0["tiles"] if tr else None,
+                "peak_source": f"{src} (sustained BF16: the kernel runs for about a second "
+                               f"inside a multi-second step)",
+                "frac_of_burst": achieved / bf16,
+                "kernel": "k_tiles_mma", "kernel_ms": tile_ms, "tiles": s0["tiles"],
+                "algorithmic_flops": head_flops,
+                "note": "head BF16 GEMM flops 2*p*n(n-1)/2 over the tile-kernel time "
+                        "(the kernel also runs the sparse FP32 tail and the epilogue)"}
+    alg_bytes = 8.0 * s0["tail_products"] + 4.0 * p * n + 12.0 * s0["candidates"]
+    achieved_gbs = alg_bytes / (tile_ms / 1e3) / 1e9
+    return {"bound": "hbm", "achieved": achieved_gbs, "peak": hbm, "unit": "GB/s",
+            "frac": achieved_gbs / hbm, "traffic": None, "peak_source": src,
+            "kernel": "k_tiles_fp32", "kernel_ms": tile_ms, "algorithmic_bytes": alg_bytes,
+            "note": "FP32 head runs on CUDA cores (FMA-bound); head FP32 FMA rate "
+                    f"{head_flops / (tile_ms / 1e3) / 1e12:.1f} TFLOP/s"}
+
+
+# DRAM bytes (read + write) of one k_tiles_mma launch per 128 x 128 tile, from
+# ncu captures of the mixed_1m shape at 200,000 rows (the full-size launch is
+# too large to capture); traffic grows with the tiles processed.
+TILE_TRAFFIC_PER_TILE = {}
+
+
+def dry_shards(args, rank, world):
+    """The multi-rank layout without a GPU: gloo ranks, each computes its
+    shard's row blocks; rank 0 checks they partition the blocks and prints
+    the line a GPU run would carry (no timing)."""
+    import datetime
+
+    import torch.distributed as dist
+
+    import cuapss
+    dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=60))
+    n = args.n or 1_000_000
+    mine = [int(b) for b in cuapss.shard_blocks(n, rank, world)]
+    objs = [None] * world
+    dist.all_gather_object(objs, mine)
+    if rank == 0:
+        nb = (n + 127) // 128
+        allb = sorted(b for o in objs for b in o)
+        tiles = [sum(nb - b for b in o) for o in objs]
+        print(json.dumps({"dry": True, "metric": METRIC, "n_gpus": world, "workload": args.workload,
+                          "n": n, "blocks": nb, "shard_blocks": [len(o) for o in objs],
+                          "shard_tiles": tiles, "partition_ok": allb == list(range(nb)),
+                          "parallelism": f"row-block shards x{world}"}))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def run_selfjoin(args, rank, world, local):
+    import numpy as np
+    import torch
+
+    import cuapss
+    from cuapss import synth
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    workload = args.workload
+    x = synth.generate(workload, n=args.n) if args.n else synth.generate(workload)
+    prec = cuapss.PREC_MIXED if args.precision == "mixed" else cuapss.PREC_FP32
+    mixed = prec == cuapss.PREC_MIXED
+    dev = {"rowptr": torch.from_numpy(x.rowptr).cuda(), "col": torch.from_numpy(x.col).cuda(),
+           "val": torch.from_numpy(x.val).cuda(), "d": x.d}
+    stream = torch.cuda.Stream()
+    pk = peaks()
+    pairs_per_step = x.n * (x.n - 1) / 2
+
+    # ---- headline: the library's configuration at --t, inputs in HBM ----
+    R = Runner(cuapss, torch, dev, local, stream, precision=prec, head_width=args.head)
+    for _ in range(max(args.warmup, 1)):
+        R.step(args.t, rank, world)
+    if dist:
+        dist.barrier()
+    clk = Clocks(local)
+    ms, stats = timed(R, torch, stream, args.t, args.steps, 0, clocks=clk, shard=rank,
+                      nshards=world)
+    if dist:
+        dist.barrier()
+        tms = torch.tensor([ms], device="cuda")
+        dist.all_reduce(tms, op=dist.ReduceOp.MAX)
+        ms = float(tms.item())
+    npairs = R.npairs
+    value = pairs_per_step / (ms / 1e3)
+    clocks = clk.summary()
+    s0 = stats[-1]
+    p = int(s0["head_width"])
+
+    # ---- end to end through the C ABI with pinned host buffers ----
+    e2e = None
+    if not args.no_e2e:
+        hp = {"rowptr": torch.from_numpy(x.rowptr).pin_memory(),
+              "col": torch.from_numpy(x.col).pin_memory(),
+              "val": torch.from_numpy(x.val).pin_memory()}
+        hcap = max(npairs, 1)
+        ho = {"i": torch.empty(hcap, dtype=torch.int32).pin_memory(),
+              "j": torch.empty(hcap, dtype=torch.int32).pin_memory(),
+              "sim": torch.empty(hcap, dtype=torch.float32).pin_memory()}
+        desc = cuapss.CsrDesc(x.n, x.d, x.nnz, hp["rowptr"].data_ptr(), hp["col"].data_ptr(),
+                              hp["val"].data_ptr(), 0)
+        L = cuapss.lib()
+
+        def hstep():
+            pr = cuapss.PairsDesc(ho["i"].data_ptr(), ho["j"].data_ptr(), ho["sim"].data_ptr(),
+                                  hcap, 0, 0)
+            if world > 1:
+                s = L.cuapss_run_shard(R.ctx._h, ctypes.byref(desc), ctypes.c_float(args.t),
+                                       rank, world, ctypes.byref(pr), None)
+            else:
+                s = L.cuapss_run(R.ctx._h, ctypes.byref(desc), ctypes.c_float(args.t),
+                                 ctypes.byref(pr), None)
+            if s != cuapss.OK:
+                raise cuapss.CuapssError(s, "cuapss_run (host buffers)")
+            return int(pr.count)
+
+        hstep()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        f0 = torch.cuda.Event(enable_timing=True)
+        f1 = torch.cuda.Event(enable_timing=True)
+        f0.record(stream)
+        for _ in range(args.steps):
+            hn = hstep()
+        f1.record(stream)
+        torch.cuda.synchronize()
+        ems = f0.elapsed_time(f1) / args.steps
+        if dist:
+            tms = torch.tensor([ems], device="cuda")
+            dist.all_reduce(tms, op=dist.ReduceOp.MAX)
+            ems = float(tms.item())
+        e2e = {"value": pairs_per_step / (ems / 1e3), "unit": "pairs/s", "ms_per_step": ems,
+               "h2d_bytes_per_step": int(x.rowptr.nbytes + x.col.nbytes + x.val.nbytes),
+               "d2h_bytes_per_step": int(hn * 12),
+               "same_pair_count": hn == npairs}
+        del hp, ho
+
+    roofline = tile_roofline(stats, p, pairs_per_step, x.n, world, mixed, x, pk)
+    line = {
+        "metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+        "dtype": "f32" if not mixed else "bf16 head + f32 tail + f64 band",
+        "data": "synthetic (seeded generator, reference corpus not distributed)",
+        "config": {"workload": workload, "n": x.n, "d": x.d, "nnz": x.nnz, "t": args.t,
+                   "precision": args.precision, "head_width": p,
+                   "named_head_width": NAMED_HEAD.get(workload),
+                   "l2": "inputs larger than L2 (CSR and head block are GBs)",
+                   "parallelism": f"row-block shards x{world}" if world > 1 else "1 GPU"},
+        "pairs_found": npairs, "candidates": s0["candidates"], "rescored": s0["rescored"],
+        "tiles": s0["tiles"], "stage_ms": mean_stage(stats),
+        "gpu_launches": int(sum(s["launches"] for s in stats)),
+        "clocks": clocks, "roofline": roofline, "e2e": e2e,
+    }
+
+    if world == 1 and not args.quick:
+        # ---- exactness against the FP64 oracle on sampled query rows ----
+        from oracle import oracle
+        ts = [tt for tt in T_SWEEP.get(workload, (args.t,))]
+        if args.t not in ts:
+            ts.append(args.t)
+        rows = sample_rows(x.n, args.check_rows, seed=12345)
+        w0 = time.time()
+        want = oracle.rows(x, min(ts), rows.astype(np.int32))
+        oracle_s = time.time() - w0
+        rows_t = torch.from_numpy(rows.astype(np.int32)).cuda()
+
+        def sampled(runner):
+            gi, gj, gs = runner.pairs()
+            sel = torch.isin(gi, rows_t) | torch.isin(gj, rows_t)
+            return gi[sel].cpu().numpy(), gj[sel].cpu().numpy(), gs[sel].cpu().numpy()
+
+        def all_pairs_sample(runner, t, k=20000):
+            gi, gj, gs = runner.pairs()
+            m = len(gi)
+            if m == 0:
+                return {"pairs": 0, "max_abs_err": 0.0, "all_at_least_t": True}
+            idx = torch.arange(0, m, max(1, m // k), device="cuda")
+            pi, pj, ps = gi[idx].cpu().numpy(), gj[idx].cpu().numpy(), gs[idx].cpu().numpy()
+            s64 = oracle.pair_sims(x, pi, pj)
+            return {"pairs": int(len(pi)), "max_abs_err": float(np.max(np.abs(ps - s64))),
+                    "all_at_least_t": bool(np.all(s64 >= t))}
+
+        chk = oracle_pairs_check(x, sampled(R), rows, want, args.t)
+        chk["oracle_s"] = oracle_s
+        chk["emitted_pairs_sample"] = all_pairs_sample(R, args.t)
+        line["oracle_check"] = chk
+
+        # ---- threshold sweep (the same configuration at the other t) ----
+        sweep = [{"t": args.t, "value": value, "ms_per_step": ms, "pairs_found": npairs,
+                  "candidates": s0["candidates"], "rescored": s0["rescored"],
+                  "oracle_check": {k: chk[k] for k in ("rows", "pairs", "pairs_equal",
+                                                       "max_abs_err")}}]
+        for tt in ts:
+            if tt == args.t:
+                continue
+            tms_, st_ = timed(R, torch, stream, tt, args.sweep_steps, 1)
+            c = oracle_pairs_check(x, sampled(R), rows, want, tt)
+            sweep.append({"t": tt, "value": pairs_per_step / (tms_ / 1e3), "ms_per_step": tms_,
+                          "pairs_found": R.npairs, "candidates": st_[-1]["candidates"],
+                          "rescored": st_[-1]["rescored"], "oracle_check": c})
+        line["t_sweep"] = sorted(sweep, key=lambda r: r["t"])
+        R.step(args.t)  # the headline's pairs again, for the comparisons below
+        head_i, head_j = R.out["i"][:npairs].clone(), R.out["j"][:npairs].clone()
+        R.close()
+
+        def same_pairs(runner):
+            return bool(runner.npairs == npairs and
+                        torch.equal(runner.out["i"][:npairs], head_i) and
+                        torch.equal(runner.out["j"][:npairs], head_j))
+
+        # ---- the head width the workload names ----
+        ph = NAMED_HEAD.get(workload)
+        if mixed and ph and ph != p and not args.no_named_head:
+            R4 = Runner(cuapss, torch, dev, local, stream, precision=prec, head_width=ph)
+            ms4, st4 = timed(R4, torch, stream, args.t, args.sweep_steps, 1)
+            line["named_head"] = {
+                "head_width": int(st4[-1]["head_width"]), "value": pairs_per_step / (ms4 / 1e3),
+                "unit": "pairs/s", "ms_per_step": ms4, "stage_ms": mean_stage(st4),
+                "same_pair_set_as_headline": same_pairs(R4),
+                "roofline": tile_roofline(st4, int(st4[-1]["head_width"]), pairs_per_step, x.n,
+                                          1, True, x, pk),
+                "note": f"the workload names a {ph}-feature dense head; the library picks "
+                        f"p = {p}, the measured optimum of tensor-core head work (2p flops per "
+                        f"pair) against sparse tail work"}
+            R4.close()
+
+        # ---- the plain FP32 hybrid on the same data ----
+        if mixed and not args.no_plain:
+            RP = Runner(cuapss, torch, dev, local, stream, precision=cuapss.PREC_FP32)
+            pms, pst = timed(RP, torch, stream, args.t, args.plain_steps, 1)
+            line["plain_fp32"] = {
+                "value": pairs_per_step / (pms / 1e3), "unit": "pairs/s", "ms_per_step": pms,
+                "steps": args.plain_steps, "head_width": int(pst[-1]["head_width"]),
+                "stage_ms": mean_stage(pst), "pairs_found": RP.npairs,
+                "same_pair_set_as_mixed": same_pairs(RP), "mixed_over_plain": pms / ms}
+            RP.close()
+        if not args.no_cpu:
+            r, h = cpu_sample(x, args.t, 128, args.cpu_budget_s)
+            h.close()
+            r.pop("sample_s", None)
+            line["cpu_baseline"] = r
+    else:
+        R.close()
+    if rank == 0:
+        print(json.dumps(line))
+    if dist:
+        dist.destroy_process_group()
 def run_batch(args, rank, world, local):
     """--workload batch: 4,096 independent instances (n log-uniform in
     [64, 20,000], d = 30,000, thresholds uniform in [0.6, 0.95]) in one
@@ -320,13 +688,13 @@ def run_batch(args, rank, world, local):
             tms = torch.tensor([ems], device="cuda")
             dist.all_reduce(tms, op=dist.ReduceOp.MAX)
             ems = float(tms.item())
-        e2e = {"value": pairs_per_step / (ems / 1e3), "unit": "pairs/s",
+        e2e = {"value": world * pairs_per_step / (ems / 1e3), "unit": "pairs/s",
                "ms_per_step": ems,
                "h2d_bytes_per_step": int(x.rowptr.nbytes + x.col.nbytes + x.val.nbytes +
                                          ipc.nbytes + tqc.nbytes),
                "d2h_bytes_per_step": int(hn * 12)}
 
-    hbm, bf16, src = peaks()
+    hbm, _, bf16, src = peaks()  # sustained BF16: the tile graph runs for ~0.2 s per step
     tile_ms = sum(s["ms_tiles"] for s in stats) / len(stats)
     s0 = stats[-1]
     tiles = int(s0["tiles"])
@@ -592,10 +960,42 @@ def run_serve(args, rank, world, local):
     print(json.dumps(line))
 
 
+def free_port() -> int:
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def launch_ranks(n: int) -> int:
+    """Re-runs this command as n ranks, one process per GPU, with the
+    environment torch.distributed.run would give them (RANK, LOCAL_RANK,
+    WORLD_SIZE, MASTER_ADDR, MASTER_PORT); returns the worst exit status. A
+    rank that fails ends the others."""
+    port = free_port()
+    procs = []
+    for r in range(n):
+        env = dict(os.environ, RANK=str(r), LOCAL_RANK=str(r), WORLD_SIZE=str(n),
+                   LOCAL_WORLD_SIZE=str(n), MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+        procs.append(subprocess.Popen([sys.executable, os.path.abspath(__file__)] + sys.argv[1:],
+                                      env=env))
+    rcs = [None] * n
+    while any(rc is None for rc in rcs):
+        for k, pr in enumerate(procs):
+            if rcs[k] is None:
+                rcs[k] = pr.poll()
+        if any(rc not in (None, 0) for rc in rcs):
+            for k, pr in enumerate(procs):
+                if rcs[k] is None:
+                    pr.terminate()
+                    rcs[k] = pr.wait()
+        time.sleep(0.2)
+    return max(abs(rc) for rc in rcs)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="cuapss", choices=["cuapss", "reference"])
     ap.add_argument("--t", type=float, default=0.7)
@@ -605,223 +1005,49 @@ def main():
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP32 comparison")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--ref-index-rows", type=int, default=100_000)
-    ap.add_argument("--ref-step-s", type=float, default=8.0)
+    ap.add_argument("--no-named-head", action="store_true",
+                    help="skip the leg at the workload's named head width")
+    ap.add_argument("--quick", action="store_true",
+                    help="headline and e2e only (no oracle check, sweep or comparisons)")
+    ap.add_argument("--sweep-steps", type=int, default=2, help="timed steps per sweep point")
+    ap.add_argument("--plain-steps", type=int, default=1, help="timed plain FP32 steps")
+    ap.add_argument("--check-rows", type=int, default=256,
+                    help="query rows checked against the FP64 oracle")
+    ap.add_argument("--cpu-budget-s", type=float, default=12.0)
+    ap.add_argument("--ref-step-s", type=float, default=4.0,
+                    help="query seconds of each reference-arm step")
     ap.add_argument("--workload", default=WORKLOAD,
-                    choices=["plain_800k", "mixed_1m", "batch", "serve"],
-                    help="plain_800k (default); mixed_1m: n = d = 1M; batch: 4,096 instances; "
+                    choices=["mixed_1m", "plain_800k", "plain_20k", "batch", "serve"],
+                    help="mixed_1m (default): n = d = 1M; plain_800k; batch: 4,096 instances; "
                          "serve: 5M-vector resident index behind the request server")
     ap.add_argument("--serve-requests", type=int, default=400)
     ap.add_argument("--k", type=int, default=4096, help="instances of the batch workload")
+    ap.add_argument("--dry-shards", action="store_true",
+                    help="CPU only: start the ranks on gloo and check the shard layout")
     args = ap.parse_args()
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        sys.exit(launch_ranks(args.gpus))
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    if args.workload == "batch" and args.impl == "cuapss":
-        run_batch(args, rank, world, local)
+    if args.dry_shards:
+        dry_shards(args, rank, world)
         return
-    if args.workload == "serve" and args.impl == "cuapss":
-        run_serve(args, rank, world, local)
-        return
-    workload = args.workload if args.workload not in ("batch", "serve") else WORKLOAD
     if args.impl == "reference":
+        if args.workload in ("batch", "serve"):
+            if rank == 0:
+                print(json.dumps({"impl": "reference", "unavailable":
+                                  "the reference has no batched or serving path"}))
+            return
         run_reference(args, rank, world)
         return
-
-    import numpy as np
-    import torch
-
-    import cuapss
-    from cuapss import synth
-
-    torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
-                                device_id=torch.device("cuda", local))
-    x = synth.generate(workload, n=args.n) if args.n else synth.generate(workload)
-    prec = cuapss.PREC_MIXED if args.precision == "mixed" else cuapss.PREC_FP32
-    dev = {"rowptr": torch.from_numpy(x.rowptr).cuda(), "col": torch.from_numpy(x.col).cuda(),
-           "val": torch.from_numpy(x.val).cuda(), "d": x.d}
-    stream = torch.cuda.Stream()
-    ctx = cuapss.Context(device=local, precision=prec, head_width=args.head,
-                         stream=stream.cuda_stream)
-    cap = 1 << 22
-    out = None
-
-    def alloc(c):
-        return {"i": torch.empty(c, dtype=torch.int32, device="cuda"),
-                "j": torch.empty(c, dtype=torch.int32, device="cuda"),
-                "sim": torch.empty(c, dtype=torch.float32, device="cuda")}
-
-    out = alloc(cap)
-
-    def step():
-        nonlocal out, cap
-        while True:
-            try:
-                if world > 1:  # this rank's shard of the one self-join
-                    return ctx.run_shard_device(dev, args.t, rank, world, out)
-                return ctx.run_device(dev, args.t, out)
-            except cuapss.CuapssError as e:
-                if e.status != cuapss.EOVERFLOW:
-                    raise
-                cap = ctx.required + 1024
-                out = alloc(cap)
-
-    for _ in range(max(args.warmup, 1)):
-        npairs = step()
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    stats = []
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    with Clocks(local) as clk:
-        e0.record(stream)
-        for _ in range(args.steps):
-            npairs = step()
-            stats.append(dict(ctx.last_stats))
-        e1.record(stream)
-        torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
-    ms = e0.elapsed_time(e1) / args.steps
-    if dist:
-        tms = torch.tensor([ms], device="cuda")
-        dist.all_reduce(tms, op=dist.ReduceOp.MAX)
-        ms = float(tms.item())
-    # the job is one self-join of x; with N ranks each evaluates its shard
-    pairs_per_step = x.n * (x.n - 1) / 2
-    value = pairs_per_step / (ms / 1e3)
-    clocks = clk.summary()
-
-    # ---- end to end through the C ABI with pinned host buffers ----
-    e2e = None
-    if not args.no_e2e:
-        hp = {"rowptr": torch.from_numpy(x.rowptr).pin_memory(),
-              "col": torch.from_numpy(x.col).pin_memory(),
-              "val": torch.from_numpy(x.val).pin_memory()}
-        hcap = max(npairs, 1)
-        ho = {"i": torch.empty(hcap, dtype=torch.int32).pin_memory(),
-              "j": torch.empty(hcap, dtype=torch.int32).pin_memory(),
-              "sim": torch.empty(hcap, dtype=torch.float32).pin_memory()}
-        desc = cuapss.CsrDesc(x.n, x.d, x.nnz, hp["rowptr"].data_ptr(), hp["col"].data_ptr(),
-                              hp["val"].data_ptr(), 0)
-        L = cuapss.lib()
-
-        def hstep():
-            pr = cuapss.PairsDesc(ho["i"].data_ptr(), ho["j"].data_ptr(), ho["sim"].data_ptr(),
-                                  hcap, 0, 0)
-            if world > 1:
-                s = L.cuapss_run_shard(ctx._h, ctypes.byref(desc), ctypes.c_float(args.t), rank,
-                                       world, ctypes.byref(pr), None)
-            else:
-                s = L.cuapss_run(ctx._h, ctypes.byref(desc), ctypes.c_float(args.t),
-                                 ctypes.byref(pr), None)
-            if s != cuapss.OK:
-                raise cuapss.CuapssError(s, "cuapss_run (host buffers)")
-            return int(pr.count)
-
-        hstep()
-        if dist:
-            dist.barrier()
-        torch.cuda.synchronize()
-        f0 = torch.cuda.Event(enable_timing=True)
-        f1 = torch.cuda.Event(enable_timing=True)
-        f0.record(stream)
-        for _ in range(args.steps):
-            hn = hstep()
-        f1.record(stream)
-        torch.cuda.synchronize()
-        ems = f0.elapsed_time(f1) / args.steps
-        if dist:
-            tms = torch.tensor([ems], device="cuda")
-            dist.all_reduce(tms, op=dist.ReduceOp.MAX)
-            ems = float(tms.item())
-        e2e = {"value": world * pairs_per_step / (ems / 1e3), "unit": "pairs/s",
-               "ms_per_step": ems,
-               "h2d_bytes_per_step": int(x.rowptr.nbytes + x.col.nbytes + x.val.nbytes),
-               "d2h_bytes_per_step": int(hn * 12)}
-
-    # ---- roofline of the dominant kernel (the pair-tile kernel) ----
-    hbm, bf16, src = peaks()
-    tile_ms = sum(s["ms_tiles"] for s in stats) / len(stats)
-    s0 = stats[-1]
-    p = int(s0["head_width"])
-    head_flops = 2.0 * p * pairs_per_step  # BF16/FP32 multiply-adds of the head dot
-    if world > 1:  # this rank's share: its tiles of the triangle's tiles
-        nb = (x.n + 127) // 128
-        head_flops *= s0["tiles"] / (nb * (nb + 1) / 2)
-    if prec == cuapss.PREC_MIXED:
-        achieved = head_flops / (tile_ms / 1e3) / 1e12
-        roofline = {"bound": "tensor", "achieved": achieved, "peak": bf16, "unit": "TFLOP/s",
-                    "frac": achieved / bf16, "traffic": None, "peak_source": src,
-                    "kernel": "k_tiles_mma", "kernel_ms": tile_ms,
-                    "algorithmic_flops": head_flops,
-                    "note": "head BF16 GEMM flops 2*p*n(n-1)/2 over the tile-kernel time "
-                            "(the kernel also runs the sparse FP32 tail and the epilogue)"}
-    else:
-        alg_bytes = 8.0 * s0["tail_products"] + 4.0 * p * x.n + 12.0 * s0["candidates"]
-        achieved_gbs = alg_bytes / (tile_ms / 1e3) / 1e9
-        roofline = {"bound": "hbm", "achieved": achieved_gbs, "peak": hbm, "unit": "GB/s",
-                    "frac": achieved_gbs / hbm, "traffic": None, "peak_source": src,
-                    "kernel": "k_tiles_fp32", "kernel_ms": tile_ms,
-                    "algorithmic_bytes": alg_bytes,
-                    "note": "FP32 head runs on CUDA cores (FMA-bound); head FP32 FMA rate "
-                            f"{head_flops / (tile_ms / 1e3) / 1e12:.1f} TFLOP/s"}
-
-    # ---- the plain FP32 hybrid on the same data (the mixed path's comparison)
-    plain = None
-    if prec == cuapss.PREC_MIXED and not args.no_plain and world == 1:
-        pctx = cuapss.Context(device=local, precision=cuapss.PREC_FP32, stream=stream.cuda_stream)
-        pout = alloc(cap)
-        pctx.run_device(dev, args.t, pout)
-        pstats = []
-        torch.cuda.synchronize()
-        g0 = torch.cuda.Event(enable_timing=True)
-        g1 = torch.cuda.Event(enable_timing=True)
-        g0.record(stream)
-        for _ in range(max(1, args.steps // 2)):
-            pn = pctx.run_device(dev, args.t, pout)
-            pstats.append(dict(pctx.last_stats))
-        g1.record(stream)
-        torch.cuda.synchronize()
-        pms = g0.elapsed_time(g1) / max(1, args.steps // 2)
-        same = bool(pn == npairs and torch.equal(pout["i"][:pn], out["i"][:npairs]) and
-                    torch.equal(pout["j"][:pn], out["j"][:npairs]))
-        plain = {"value": pairs_per_step / (pms / 1e3), "unit": "pairs/s",
-                 "ms_per_step": pms, "head_width": int(pstats[-1]["head_width"]),
-                 "pairs_found": pn, "same_pair_set_as_mixed": same,
-                 "mixed_over_plain": pms / ms}
-        pctx.close()
-
-    line = {
-        "metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
-        "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
-        "dtype": "f32" if prec == cuapss.PREC_FP32 else "bf16 head + f32 tail + f64 band",
-        "data": "synthetic (seeded generator, reference corpus not distributed)",
-        "config": {"workload": workload, "n": x.n, "d": x.d, "nnz": x.nnz, "t": args.t,
-                   "precision": args.precision, "head_width": p,
-                   "l2": "inputs larger than L2 (CSR + head block > 126 MB)",
-                   "parallelism": f"row-block shards x{world}" if world > 1 else "1 GPU"},
-        "pairs_found": npairs, "candidates": s0["candidates"], "rescored": s0["rescored"],
-        "stage_ms": {k: sum(s[k] for s in stats) / len(stats)
-                     for k in ("ms_preprocess", "ms_tiles", "ms_finalize", "ms_total")},
-        "gpu_launches": int(sum(s["launches"] for s in stats)),
-        "clocks": clocks, "roofline": roofline, "e2e": e2e, "plain_fp32": plain,
-    }
-    if rank == 0 and world == 1 and not args.no_cpu:
-        line["cpu_baseline"] = cpu_baseline(x, args.t, 128)  # the CPU's own best head width
-    if rank == 0:
-        print(json.dumps(line))
-    ctx.close()
-    if dist:
-        dist.destroy_process_group()
+    if args.workload == "batch":
+        run_batch(args, rank, world, local)
+        return
+    if args.workload == "serve":
+        run_serve(args, rank, world, local)
+        return
+    run_selfjoin(args, rank, world, local)
 
 
 if __name__ == "__main__":

@@ -42,7 +42,7 @@
 extern "C" {
 #endif
 
-#define CUAPSS_ABI_VERSION 1
+#define CUAPSS_ABI_VERSION 2
 
 typedef enum {
   CUAPSS_OK = 0,
@@ -152,15 +152,16 @@ int32_t cuapss_shard_blocks(int64_t n, int32_t shard, int32_t nshards, int32_t* 
                             int64_t capacity);
 
 /* Self-check of failure detection: every device wait of the tile kernels is
- * bounded (mbarrier try-wait with a poll limit, about 2 s) and reports
- * CUAPSS_ETIMEOUT instead of hanging. This runs a kernel that waits, with the
- * same primitive and at most max_polls polls (1 .. 100000), on a barrier that
- * nothing completes; it returns CUAPSS_ETIMEOUT when the wait gave up and
- * reported it as designed (any other status is a failure), and *polls_done
- * (may be NULL) the polls made. The context stays usable. No counterpart in
- * the reference, whose waits are blocking host syncs. */
-cuapss_status cuapss_selftest_bounded_wait(cuapss_ctx* ctx, int32_t max_polls,
-                                           int32_t* polls_done);
+ * bounded by device time (mbarrier try-wait against a %globaltimer deadline
+ * of 2 s) and reports CUAPSS_ETIMEOUT instead of hanging. This runs a kernel
+ * that waits, with the same primitive and a deadline of limit_us
+ * microseconds (1 .. 2,000,000), on a barrier that nothing completes; it
+ * returns CUAPSS_ETIMEOUT when the wait gave up and reported it as designed
+ * (any other status is a failure), and *waited_ns (may be NULL) the device
+ * time from the first poll to the give-up. The context stays usable. No
+ * counterpart in the reference, whose waits are blocking host syncs. */
+cuapss_status cuapss_selftest_bounded_wait(cuapss_ctx* ctx, int32_t limit_us,
+                                           int64_t* waited_ns);
 
 /* Cross-join: all pairs (a, b), a row of `a`, b row of `b`, sim >= t.
  * out->i holds the row of `a`, out->j the row of `b`; sorted by (i, j).
@@ -318,9 +319,12 @@ cuapss_status cuapss_feature_remap(cuapss_ctx* ctx, const cuapss_csr* x,
  * path forbids cudaMalloc/cudaFree. x, perm and counts must be device
  * pointers on ctx's device (x->on_device = 1); all other memory is a fixed
  * ~1.6 MB file-scope device array, so d <= 65536 (larger d: CUAPSS_EINVAL).
- * The first call on a device looks up that array's address and should come
- * before any stream capture. Calls that overlap on the GPU share the array
- * and race: serialise them. No counterpart in the reference. */
+ * Each call looks up that array's address on its device; the first call on a
+ * device can load the module and should come before any stream capture. The
+ * call returns once its work on ctx's stream is done (the host waits for it).
+ * Calls that overlap on the GPU share the array and race: serialise them. If
+ * the call returns CUAPSS_EINVAL for a bad column id or an unsorted row,
+ * perm and counts are undefined. No counterpart in the reference. */
 cuapss_status cuapss_feature_remap_noalloc(cuapss_ctx* ctx, const cuapss_csr* x,
                                            int32_t* perm, int32_t* counts);
 

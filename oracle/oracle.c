@@ -352,14 +352,29 @@ static int cmp_ent(const void* a, const void* b) {
   return (x > y) - (x < y);
 }
 
-int64_t cpu_hybrid_apss(int64_t n, int64_t d, const int64_t* rowptr,
-                        const int32_t* col, const float* val, float t,
-                        int32_t p, int64_t q0, int64_t q1, int threads,
-                        double* sec_prep, double* sec_query) {
-  if (!valid_csr(n, d, rowptr, col) || p < 0) return -1;
+struct cpu_hybrid {
+  int64_t n;
+  int32_t p;
+  const int64_t* rowptr;
+  ent_t* ent;    /* remapped entries, each row sorted by rank */
+  int64_t* hend; /* end of each row's head (rank < p) prefix */
+  float* hn;     /* FP32 head norms */
+  int64_t* tptr; /* tail inverted lists, rows ascending */
+  int32_t* trow;
+  float* tval;
+};
+
+cpu_hybrid_t* cpu_hybrid_prepare(int64_t n, int64_t d, const int64_t* rowptr,
+                                 const int32_t* col, const float* val,
+                                 int32_t p, int threads, double* sec_prep) {
+  if (!valid_csr(n, d, rowptr, col) || p < 0) return NULL;
   if (threads > 0) omp_set_num_threads(threads);
   const double w0 = omp_get_wtime();
   const int64_t nnz = rowptr[n];
+  cpu_hybrid_t* h = (cpu_hybrid_t*)calloc(1, sizeof(cpu_hybrid_t));
+  h->n = n;
+  h->p = p;
+  h->rowptr = rowptr;
   /* frequency remap and per-row re-sort: head = rank < p is a row prefix */
   int32_t* perm = (int32_t*)malloc(sizeof(int32_t) * (size_t)(d > 0 ? d : 1));
   int32_t* cnt = (int32_t*)malloc(sizeof(int32_t) * (size_t)(d > 0 ? d : 1));
@@ -370,15 +385,15 @@ int64_t cpu_hybrid_apss(int64_t n, int64_t d, const int64_t* rowptr,
 #pragma omp parallel for schedule(dynamic, 256)
   for (int64_t i = 0; i < n; ++i) {
     double ss = 0.0;
-    int64_t h = rowptr[i];
+    int64_t hh = rowptr[i];
     for (int64_t e = rowptr[i]; e < rowptr[i + 1]; ++e) {
       ent[e].c = perm[col[e]];
       ent[e].v = val[e];
     }
     qsort(ent + rowptr[i], (size_t)(rowptr[i + 1] - rowptr[i]), sizeof(ent_t), cmp_ent);
-    for (int64_t e = rowptr[i]; e < rowptr[i + 1] && ent[e].c < p; ++e, ++h)
+    for (int64_t e = rowptr[i]; e < rowptr[i + 1] && ent[e].c < p; ++e, ++hh)
       ss += (double)ent[e].v * ent[e].v;
-    hend[i] = h;
+    hend[i] = hh;
     hn[i] = (float)sqrt(ss);
   }
   /* tail inverted lists (rows ascending) */
@@ -398,22 +413,49 @@ int64_t cpu_hybrid_apss(int64_t n, int64_t d, const int64_t* rowptr,
       tval[k] = ent[e].v;
     }
   free(cur);
-  const double w1 = omp_get_wtime();
+  free(perm);
+  free(cnt);
+  h->ent = ent;
+  h->hend = hend;
+  h->hn = hn;
+  h->tptr = tptr;
+  h->trow = trow;
+  h->tval = tval;
+  if (sec_prep) *sec_prep = omp_get_wtime() - w0;
+  return h;
+}
+
+int64_t cpu_hybrid_query(const cpu_hybrid_t* h, float t, int64_t m,
+                         const int64_t* qrows, int64_t q0, int threads,
+                         double* sec_query) {
+  if (!h) return -1;
+  if (threads > 0) omp_set_num_threads(threads);
+  const double w0 = omp_get_wtime();
+  const int64_t n = h->n;
+  const int32_t p = h->p;
+  const int64_t* rowptr = h->rowptr;
+  const ent_t* ent = h->ent;
+  const int64_t* hend = h->hend;
+  const float* hn = h->hn;
+  const int64_t* tptr = h->tptr;
+  const int32_t* trow = h->trow;
+  const float* tval = h->tval;
   int64_t found = 0;
-  if (q1 > n) q1 = n;
 #pragma omp parallel reduction(+ : found)
   {
     float* acc = (float*)calloc((size_t)(n > 0 ? n : 1), sizeof(float));
     float* q = (float*)calloc((size_t)(p > 0 ? p : 1), sizeof(float));
 #pragma omp for schedule(dynamic, 1)
-    for (int64_t i = q0; i < q1; ++i) {
+    for (int64_t k = 0; k < m; ++k) {
+      const int64_t i = qrows ? qrows[k] : q0 + k;
+      if (i < 0 || i >= n) continue;
       /* tail: feature-parallel accumulation through inverted lists */
       for (int64_t e = hend[i]; e < rowptr[i + 1]; ++e) {
         const int32_t f = ent[e].c;
         const float x = ent[e].v;
-        for (int64_t k = upper_bound_i32(trow, tptr[f], tptr[f + 1], (int32_t)i);
-             k < tptr[f + 1]; ++k)
-          acc[trow[k]] += x * tval[k];
+        for (int64_t r = upper_bound_i32(trow, tptr[f], tptr[f + 1], (int32_t)i);
+             r < tptr[f + 1]; ++r)
+          acc[trow[r]] += x * tval[r];
       }
       for (int64_t e = rowptr[i]; e < hend[i]; ++e) q[ent[e].c] = ent[e].v;
       const float hi = hn[i];
@@ -430,16 +472,31 @@ int64_t cpu_hybrid_apss(int64_t n, int64_t d, const int64_t* rowptr,
     free(acc);
     free(q);
   }
-  const double w2 = omp_get_wtime();
-  if (sec_prep) *sec_prep = w1 - w0;
-  if (sec_query) *sec_query = w2 - w1;
-  free(perm);
-  free(cnt);
-  free(ent);
-  free(hend);
-  free(hn);
-  free(tptr);
-  free(trow);
-  free(tval);
+  if (sec_query) *sec_query = omp_get_wtime() - w0;
+  return found;
+}
+
+void cpu_hybrid_free(cpu_hybrid_t* h) {
+  if (!h) return;
+  free(h->ent);
+  free(h->hend);
+  free(h->hn);
+  free(h->tptr);
+  free(h->trow);
+  free(h->tval);
+  free(h);
+}
+
+int64_t cpu_hybrid_apss(int64_t n, int64_t d, const int64_t* rowptr,
+                        const int32_t* col, const float* val, float t,
+                        int32_t p, int64_t q0, int64_t q1, int threads,
+                        double* sec_prep, double* sec_query) {
+  cpu_hybrid_t* h = cpu_hybrid_prepare(n, d, rowptr, col, val, p, threads, sec_prep);
+  if (!h) return -1;
+  if (q1 > n) q1 = n;
+  if (q0 < 0) q0 = 0;
+  const int64_t found =
+      cpu_hybrid_query(h, t, q1 > q0 ? q1 - q0 : 0, NULL, q0, threads, sec_query);
+  cpu_hybrid_free(h);
   return found;
 }

@@ -89,6 +89,18 @@ int64_t cpu_hybrid_apss(int64_t n, int64_t d, const int64_t* rowptr,
                         int32_t p, int64_t q0, int64_t q1, int threads,
                         double* sec_prep, double* sec_query);
 
+/* The same baseline split in two: the preprocessing once (the handle keeps
+ * pointers to rowptr, which must outlive it), then queries over any rows:
+ * qrows[0..m) when qrows is non-NULL, else rows q0 .. q0 + m - 1. */
+typedef struct cpu_hybrid cpu_hybrid_t;
+cpu_hybrid_t* cpu_hybrid_prepare(int64_t n, int64_t d, const int64_t* rowptr,
+                                 const int32_t* col, const float* val,
+                                 int32_t p, int threads, double* sec_prep);
+int64_t cpu_hybrid_query(const cpu_hybrid_t* h, float t, int64_t m,
+                         const int64_t* qrows, int64_t q0, int threads,
+                         double* sec_query);
+void cpu_hybrid_free(cpu_hybrid_t* h);
+
 /* Threads OpenMP will use for threads <= 0. */
 int oracle_max_threads(void);
 

@@ -47,6 +47,14 @@ def lib():
                                       _i64, _i64, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
                                       ctypes.POINTER(ctypes.c_double)]
         L.cpu_hybrid_apss.restype = _i64
+        L.cpu_hybrid_prepare.argtypes = [_i64, _i64, _p, _p, _p, ctypes.c_int32, ctypes.c_int,
+                                         ctypes.POINTER(ctypes.c_double)]
+        L.cpu_hybrid_prepare.restype = ctypes.c_void_p
+        L.cpu_hybrid_query.argtypes = [ctypes.c_void_p, ctypes.c_float, _i64, _p, _i64,
+                                       ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
+        L.cpu_hybrid_query.restype = _i64
+        L.cpu_hybrid_free.argtypes = [ctypes.c_void_p]
+        L.cpu_hybrid_free.restype = None
         L.oracle_max_threads.restype = ctypes.c_int
         _lib = L
     return _lib
@@ -129,6 +137,43 @@ def cpu_hybrid(x, t: float, p: int, q0: int, q1: int, threads: int = 0):
     if c < 0:
         raise ValueError("cpu_hybrid rejected the input")
     return int(c), sp.value, sq.value
+
+
+class CpuHybrid:
+    """The OpenMP FP32 hybrid with its preprocessing done once: prep_s holds
+    its wall seconds; query(t, rows) counts the pairs (i, j > i) of the given
+    query rows and returns (count, seconds)."""
+
+    def __init__(self, x, p: int, threads: int = 0):
+        self._x = x  # the handle points into x's arrays
+        self.threads = int(threads)
+        sp = ctypes.c_double()
+        self._h = lib().cpu_hybrid_prepare(x.n, x.d, x.rowptr.ctypes.data, x.col.ctypes.data,
+                                           x.val.ctypes.data, int(p), self.threads,
+                                           ctypes.byref(sp))
+        if not self._h:
+            raise ValueError("cpu_hybrid_prepare rejected the input")
+        self.prep_s = sp.value
+
+    def query(self, t: float, rows):
+        r = np.ascontiguousarray(rows, dtype=np.int64)
+        sq = ctypes.c_double()
+        c = lib().cpu_hybrid_query(self._h, float(t), len(r), r.ctypes.data, 0, self.threads,
+                                   ctypes.byref(sq))
+        if c < 0:
+            raise ValueError("cpu_hybrid_query failed")
+        return int(c), sq.value
+
+    def close(self):
+        if self._h:
+            lib().cpu_hybrid_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def max_threads() -> int:

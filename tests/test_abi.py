@@ -42,7 +42,7 @@ def test_synth_symbols_exported():
 
 
 def test_status_strings_and_defaults():
-    assert cuapss.lib().cuapss_abi_version() == 1
+    assert cuapss.lib().cuapss_abi_version() == 2
     assert cuapss.status_string(cuapss.OK) == "ok"
     assert "capacity" in cuapss.status_string(cuapss.EOVERFLOW)
     o = cuapss.default_opts()

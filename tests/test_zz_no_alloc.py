@@ -1,6 +1,7 @@
 """cuapss_feature_remap_noalloc (the allocation-free frequency remap) called
-through the C ABI with CUDA buffers, checked against cuapss_feature_remap on
-the same inputs. Integer outputs, so the tolerance is exact equality.
+through the C ABI with CUDA buffers, checked against cuapss_feature_remap and
+the CPU oracle's remap on the same inputs. Integer outputs, so the tolerance
+is exact equality.
 
 The file name sorts last so that the test also runs after every other test
 in one process (the scratch array then holds earlier calls' leftovers)."""
@@ -11,6 +12,7 @@ import pytest
 
 import cuapss
 from cuapss import synth
+from oracle import oracle
 
 pytestmark = pytest.mark.gpu
 
@@ -63,6 +65,10 @@ def test_noalloc_matches_remap_twice(torch_cuda, cfg, n, d):
             torch.cuda.synchronize()
             np.testing.assert_array_equal(counts.cpu().numpy(), want_counts)
             np.testing.assert_array_equal(perm.cpu().numpy(), want_perm)
+            # and directly against the oracle's remap
+            o_perm, o_counts = oracle.feature_remap(inp)
+            np.testing.assert_array_equal(counts.cpu().numpy(), o_counts)
+            np.testing.assert_array_equal(perm.cpu().numpy(), o_perm)
             # a permutation of 0..d-1 ordered by (count desc, id asc)
             p = perm.cpu().numpy()
             order = np.argsort(p)
