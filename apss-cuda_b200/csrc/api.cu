@@ -134,7 +134,6 @@ cuapss_status join_device(cuapss_ctx* ctx, const DevCsr& a, const DevCsr* b, flo
   // Rows keep the caller's order: a 128-row block of random rows carries a
   // near-average tail, so the tail's shared-memory staging fits almost every
   // block (grouping long rows together would overflow it).
-  po.row_sort = 0;
   po.want_head32 = mixed ? 0 : 1;
   po.want_head16 = mixed ? 1 : 0;
   Side SA, SB;

@@ -167,7 +167,6 @@ cuapss_status prepare_bucket(cuapss_ctx* ctx, const BatchIn& in, Bucket& b, int 
   // ---- side
   PrepOptions po;
   po.p = p;
-  po.row_sort = 0;  // slots keep their order: blocks never straddle instances
   po.want_head32 = in.mixed ? 0 : 1;
   po.want_head16 = in.mixed ? 1 : 0;
   b.S = Side{};

@@ -53,6 +53,11 @@ enum : int {
 };
 
 constexpr int kBlockRows = 128;  // rows per row block (tile edge)
+// The J side's tail postings are kept per segment of kJSegRows rows (kJSegs
+// per row block), each sorted by feature: the tile kernels run a tile's tail
+// one segment (a slab of kJSegRows tile columns) at a time.
+constexpr int kJSegRows = 32;
+constexpr int kJSegs = kBlockRows / kJSegRows;
 // Tail staging capacity of the tile kernels: a block's feature groups are
 // staged in shared memory in chunks of at most this many groups / postings.
 // Tail postings of a row block are bucketed by the low kTailBucketBits bits

@@ -2,7 +2,10 @@
 // tile-ELL partitions in, one exact self-join over their union, pair counts
 // per partition pair printed in the reference's format.
 #include <algorithm>
+#include <cerrno>
 #include <cstdio>
+#include <cstdlib>
+#include <cstring>
 #include <mutex>
 #include <numeric>
 #include <utility>
@@ -61,6 +64,107 @@ extern "C" int64_t cuapss_compat_tile_ell_to_csr(const int* dim, const float* fe
     rowptr[v + 1] = nnz;
   }
   return nnz;
+}
+
+namespace {
+
+// Parses the reference's text format (one vector per line, see
+// cuapss_compat.h). For each vector calls row(entries); stops after
+// max_rows vectors when max_rows >= 0. Returns false on a malformed line.
+template <typename Row>
+bool parse_text(const char* path, int64_t max_rows, Row row) {
+  FILE* f = std::fopen(path, "rb");
+  if (!f) return false;
+  std::vector<char> line;
+  std::vector<std::pair<int32_t, float>> ent;
+  bool ok = true;
+  int64_t rows = 0;
+  for (;;) {
+    if (max_rows >= 0 && rows >= max_rows) break;
+    line.clear();
+    int c;
+    while ((c = std::fgetc(f)) != EOF && c != '\n') line.push_back((char)c);
+    if (c == EOF && line.empty()) break;  // end of file (no partial last vector)
+    line.push_back('\0');
+    ent.clear();
+    // the reference consumes one character, then reads pairs while the
+    // character after a pair is not the newline
+    const char* q = line.size() > 1 ? line.data() + 1 : line.data() + line.size() - 1;
+    while (*q) {
+      char* e1 = nullptr;
+      errno = 0;
+      const long long d = std::strtoll(q, &e1, 10);
+      if (e1 == q || errno || d < 0 || d > INT32_MAX) { ok = false; break; }
+      char* e2 = nullptr;
+      const float v = std::strtof(e1, &e2);
+      if (e2 == e1) { ok = false; break; }
+      ent.emplace_back((int32_t)d, v);
+      q = e2;
+      if (*q) ++q;  // the one character after the pair
+    }
+    if (!ok) break;
+    std::sort(ent.begin(), ent.end(),
+              [](const std::pair<int32_t, float>& a, const std::pair<int32_t, float>& b) {
+                return a.first < b.first;
+              });
+    for (size_t m = 1; m < ent.size(); ++m)
+      if (ent[m].first == ent[m - 1].first) ok = false;
+    if (!ok) break;
+    row(ent);
+    ++rows;
+    if (c == EOF) break;
+  }
+  std::fclose(f);
+  return ok;
+}
+
+}  // namespace
+
+extern "C" int cuapss_compat_text_size(const char* path, int64_t max_rows, int64_t* n_rows,
+                                       int64_t* nnz, int64_t* d) {
+  if (!path || !n_rows || !nnz || !d) return -1;
+  int64_t n = 0, m = 0, dmax = 0;
+  const bool ok = parse_text(path, max_rows, [&](const std::vector<std::pair<int32_t, float>>& e) {
+    ++n;
+    m += (int64_t)e.size();
+    if (!e.empty()) dmax = std::max<int64_t>(dmax, (int64_t)e.back().first + 1);
+  });
+  if (!ok) return -1;
+  *n_rows = n;
+  *nnz = m;
+  *d = dmax;
+  return 0;
+}
+
+extern "C" int cuapss_compat_read_text(const char* path, int64_t max_rows, int64_t* rowptr,
+                                       int32_t* col, float* val) {
+  if (!path || !rowptr) return -1;
+  int64_t n = 0, m = 0;
+  rowptr[0] = 0;
+  const bool ok = parse_text(path, max_rows, [&](const std::vector<std::pair<int32_t, float>>& e) {
+    for (const auto& pr : e) {
+      col[m] = pr.first;
+      val[m] = pr.second;
+      ++m;
+    }
+    rowptr[++n] = m;
+  });
+  return ok ? 0 : -1;
+}
+
+extern "C" int cuapss_compat_write_text(const char* path, int64_t n, const int64_t* rowptr,
+                                        const int32_t* col, const float* val) {
+  if (!path || n < 0 || (n > 0 && !rowptr)) return -1;
+  FILE* f = std::fopen(path, "wb");
+  if (!f) return -1;
+  bool ok = true;
+  for (int64_t r = 0; r < n && ok; ++r) {
+    for (int64_t e = rowptr[r]; e < rowptr[r + 1] && ok; ++e)
+      ok = std::fprintf(f, " %d %.9g", (int)col[e], (double)val[e]) > 0;
+    ok = ok && std::fputc('\n', f) != EOF;
+  }
+  ok = (std::fclose(f) == 0) && ok;
+  return ok ? 0 : -1;
 }
 
 extern "C" void cuapss_compat_set_threshold(float t) {

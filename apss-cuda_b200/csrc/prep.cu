@@ -1,4 +1,4 @@
-// Validation, frequency remap, row ordering, head block and inverted-list
+// Validation, frequency remap, head block and inverted-list
 // build for one join operand.
 //
 // Reference counterparts (fengyilin118/APSS-CUDA):
@@ -60,19 +60,60 @@ __global__ void k_check_rowptr(const int64_t* __restrict__ rp, int64_t n, int64_
 }
 
 // One warp per row: id range/order, finite values, FP64 norm, posting counts.
-// Posting counts of up to kHistMax features are first gathered in a per-CTA
-// shared-memory histogram (hot Zipf features would otherwise serialize on
-// one global counter), then added to counts once per CTA.
+// Hot Zipf features would serialize on their global counters, so counts are
+// first gathered per CTA in shared memory and added to the global counts
+// once per CTA:
+//   kHistDirect: d <= kHistMax, one shared counter per feature;
+//   kHistHashed: larger d, a shared hash table of kHashSlots (feature,
+//     count) slots, open addressing with kHashProbes probes; the hot features
+//     take their slots early and stay there, an entry whose probes all find
+//     other features goes to its global counter;
+//   kHistGlobal: global atomics only (small inputs).
 constexpr int64_t kHistMax = 50176;
+constexpr int kHashBits = 14;
+constexpr int kHashSlots = 1 << kHashBits;  // 128 KB: keys + counts
+constexpr int kHashProbes = 4;
+constexpr uint32_t kHashEmpty = 0xffffffffu;
+enum HistMode { kHistGlobal = 0, kHistDirect = 1, kHistHashed = 2 };
 
-template <bool SMEM_HIST>
+__device__ __forceinline__ void hist_add(int mode, int* hist, int32_t* __restrict__ counts,
+                                         int32_t c) {
+  if (mode == kHistDirect) {
+    atomicAdd(&hist[c], 1);
+    return;
+  }
+  if (mode == kHistHashed) {
+    uint32_t* hk = reinterpret_cast<uint32_t*>(hist);
+    int* hc = hist + kHashSlots;
+    const uint32_t h = ((uint32_t)c * 2654435761u) >> (32 - kHashBits);
+#pragma unroll
+    for (int q = 0; q < kHashProbes; ++q) {
+      const uint32_t slot = (h + (uint32_t)q) & (kHashSlots - 1u);
+      uint32_t k = hk[slot];
+      if (k == kHashEmpty) k = atomicCAS(&hk[slot], kHashEmpty, (uint32_t)c);
+      if (k == kHashEmpty || k == (uint32_t)c) {
+        atomicAdd(&hc[slot], 1);
+        return;
+      }
+    }
+  }
+  atomicAdd(&counts[c], 1);
+}
+
+template <int MODE>
 __global__ void k_check_rows(const int64_t* __restrict__ rp, const int32_t* __restrict__ col,
                              const float* __restrict__ val, int64_t n, int64_t d, float tol,
                              int check, int32_t* __restrict__ counts, int* err,
                              unsigned long long* nrm_max_bits) {
   extern __shared__ int hist[];
-  if (SMEM_HIST) {
+  if (MODE == kHistDirect) {
     for (int64_t f = threadIdx.x; f < d; f += blockDim.x) hist[f] = 0;
+    __syncthreads();
+  } else if (MODE == kHistHashed) {
+    for (int k = threadIdx.x; k < kHashSlots; k += blockDim.x) {
+      hist[k] = (int)kHashEmpty;
+      hist[kHashSlots + k] = 0;
+    }
     __syncthreads();
   }
   const int lane = threadIdx.x & 31;
@@ -90,10 +131,7 @@ __global__ void k_check_rows(const int64_t* __restrict__ rp, const int32_t* __re
       if (e > lo && col[e - 1] >= c) bad |= kErrColOrder;
       if (!isfinite(v)) bad |= kErrValue;
       ss += (double)v * (double)v;
-      if (counts && c >= 0 && c < d) {
-        if (SMEM_HIST) atomicAdd(&hist[c], 1);
-        else atomicAdd(&counts[c], 1);
-      }
+      if (counts && c >= 0 && c < d) hist_add(MODE, hist, counts, c);
     }
     ss = warp_sum_d(ss);
     bad = warp_or(bad);
@@ -106,11 +144,16 @@ __global__ void k_check_rows(const int64_t* __restrict__ rp, const int32_t* __re
     if (bad_all) atomicOr(err, bad_all);
     if (nrm_max > 0.0) atomicMax(nrm_max_bits, (unsigned long long)__double_as_longlong(nrm_max));
   }
-  if (SMEM_HIST) {
+  if (MODE == kHistDirect) {
     __syncthreads();
     if (counts)
       for (int64_t f = threadIdx.x; f < d; f += blockDim.x)
         if (hist[f]) atomicAdd(&counts[f], hist[f]);
+  } else if (MODE == kHistHashed) {
+    __syncthreads();
+    if (counts)
+      for (int k = threadIdx.x; k < kHashSlots; k += blockDim.x)
+        if (hist[kHashSlots + k]) atomicAdd(&counts[hist[k]], hist[kHashSlots + k]);
   }
 }
 
@@ -136,150 +179,69 @@ __global__ void k_iota_i32(int32_t* v, int64_t n) {
     v[i] = (int32_t)i;
 }
 
-__global__ void k_row_keys(const int64_t* __restrict__ rp, int64_t n, int64_t d, int rbits,
-                           uint64_t* __restrict__ keys, uint32_t* __restrict__ vals) {
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t len = rp[i + 1] - rp[i];
-    keys[i] = ((uint64_t)(d - len) << rbits) | (uint64_t)i;
-    vals[i] = (uint32_t)i;
-  }
-}
-
-__global__ void k_rowperm(const uint32_t* __restrict__ sorted_rows, const int64_t* __restrict__ rp,
-                          int64_t n, int32_t* __restrict__ rowperm, int32_t* __restrict__ rowinv,
-                          int64_t* __restrict__ newlen) {
-  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n;
-       r += (int64_t)gridDim.x * blockDim.x) {
-    const int32_t old = (int32_t)sorted_rows[r];
-    rowperm[r] = old;
-    rowinv[old] = (int32_t)r;
-    newlen[r] = rp[old + 1] - rp[old];
-  }
-}
-
-// One warp per caller row: key (new row, remapped feature) per entry.
-__global__ void k_entry_keys(const int64_t* __restrict__ rp, const int32_t* __restrict__ col,
-                             const int32_t* __restrict__ perm, const int32_t* __restrict__ rowinv,
-                             int64_t n, int fbits, uint64_t* __restrict__ keys,
-                             uint32_t* __restrict__ vals) {
-  const int lane = threadIdx.x & 31;
-  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
-  for (int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; i < n; i += warps) {
-    const uint64_t r = (uint64_t)rowinv[i];
-    for (int64_t e = rp[i] + lane; e < rp[i + 1]; e += 32) {
-      keys[e] = (r << fbits) | (uint64_t)perm[col[e]];
-      vals[e] = (uint32_t)e;
-    }
-  }
-}
-
-// Remapped ids of each row split into its head (rank < p, written forward
-// from the row's start) and its tail (written backward from its end), one
-// warp per row, rows in input order. Nothing downstream depends on the order
-// inside either part: the head block is a dense scatter, and the tail lists
-// are built by stable sorts on (block, feature) / (half-block, feature), which
-// see the rows in order.
+// One warp per row, one pass over the caller's CSR: feature ids remapped to
+// their frequency rank; the head entries (rank < p) scattered straight into
+// the dense head block (BF16 tiles in the tensor core's swizzled layout,
+// and/or FP32 k-major slices) and summed into the FP64 head norm; the tail
+// entries (rank >= p) written, remapped, to the end of the row's range in
+// col2/val2 (a suffix of length tcount[r]; the head part of col2/val2 is not
+// written); per-row nnz, head length and the block's largest nnz. Rows keep
+// the caller's order. Nothing downstream depends on the order inside the
+// tail suffix: the tail lists are built by sorts on (block, feature) and
+// (J segment, feature).
+//
+// BF16 tile layout: one 16 KB tile per (row block, 64-feature chunk); row rr
+// of the tile occupies bytes [128 rr, 128 rr + 128) and its 16-byte chunk c
+// (features 8c..8c+7 of the chunk) sits at chunk position c ^ (rr % 8), the
+// 128-byte swizzle the tensor core expects, so a plain bulk copy lands a tile
+// in shared memory ready for tcgen05.mma. FP32 layout: head32[b][f][rr].
 __global__ void k_split_rows(const int64_t* __restrict__ rp, const int32_t* __restrict__ col,
                              const float* __restrict__ val, const int32_t* __restrict__ perm,
                              int64_t n, int p, int32_t* __restrict__ col2,
-                             float* __restrict__ val2) {
+                             float* __restrict__ val2, int32_t* __restrict__ hlen,
+                             int32_t* __restrict__ nnz_row, float* __restrict__ hnorm,
+                             int64_t* __restrict__ tcount, int32_t* __restrict__ blk_maxnnz,
+                             __nv_bfloat16* __restrict__ head16, int nkc,
+                             float* __restrict__ head32) {
   const int lane = threadIdx.x & 31;
   const unsigned lt = (1u << lane) - 1u;
   const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
   for (int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; i < n; i += warps) {
     const int64_t lo = rp[i], hi = rp[i + 1];
+    const int64_t b = i / kBlockRows, rr = i % kBlockRows;
     int64_t nh = 0, nt = 0;
+    double hs = 0.0;
     for (int64_t base = lo; base < hi; base += 32) {
       const int64_t e = base + lane;
       const bool valid = e < hi;
       const int32_t rank = valid ? perm[col[e]] : 0;
       const float v = valid ? val[e] : 0.0f;
-      const unsigned hb = __ballot_sync(0xffffffffu, valid && rank < p);
-      const unsigned tb = __ballot_sync(0xffffffffu, valid && rank >= p);
-      if (valid) {
-        const int64_t dst = rank < p ? lo + nh + __popc(hb & lt) : hi - 1 - (nt + __popc(tb & lt));
+      const bool head = valid && rank < p;
+      const unsigned tb = __ballot_sync(0xffffffffu, valid && !head);
+      if (head) {
+        hs += (double)v * (double)v;
+        if (head16) {
+          const int kc = rank >> 6, c = (rank >> 3) & 7, w = rank & 7;
+          const int64_t off =
+              (((b * nkc + kc) * kBlockRows + rr) * 128 + ((c ^ (int)(rr & 7)) * 16)) / 2 + w;
+          head16[off] = __float2bfloat16_rn(v);
+        }
+        if (head32) head32[(b * p + rank) * kBlockRows + rr] = v;
+      } else if (valid) {
+        const int64_t dst = hi - 1 - (nt + __popc(tb & lt));
         col2[dst] = rank;
         val2[dst] = v;
       }
-      nh += __popc(hb);
+      nh += __popc(__ballot_sync(0xffffffffu, head));
       nt += __popc(tb);
     }
-  }
-}
-
-__global__ void k_gather_entries(const uint64_t* __restrict__ keys, const uint32_t* __restrict__ src,
-                                 const float* __restrict__ val, int64_t nnz, uint64_t fmask,
-                                 int32_t* __restrict__ col2, float* __restrict__ val2) {
-  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < nnz;
-       k += (int64_t)gridDim.x * blockDim.x) {
-    col2[k] = (int32_t)(keys[k] & fmask);
-    val2[k] = val[src[k]];
-  }
-}
-
-// One warp per new row: head length, FP64 head norm, block max nnz.
-__global__ void k_row_stats(const int64_t* __restrict__ rp2, const int32_t* __restrict__ col2,
-                            const float* __restrict__ val2, int64_t n, int p,
-                            int32_t* __restrict__ hlen, int32_t* __restrict__ nnz_row,
-                            float* __restrict__ hnorm, int64_t* __restrict__ tcount,
-                            int32_t* __restrict__ blk_maxnnz) {
-  const int lane = threadIdx.x & 31;
-  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
-  for (int64_t r = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; r < n; r += warps) {
-    const int64_t lo = rp2[r], hi = rp2[r + 1];
-    int hl = 0;
-    double hs = 0.0;
-    for (int64_t e = lo + lane; e < hi; e += 32) {
-      if (col2[e] < p) {
-        ++hl;
-        hs += (double)val2[e] * (double)val2[e];
-      }
-    }
-    hl = warp_sum_i(hl);
     hs = warp_sum_d(hs);
     if (lane == 0) {
-      hlen[r] = hl;
-      nnz_row[r] = (int32_t)(hi - lo);
-      hnorm[r] = __double2float_ru(sqrt(hs));
-      tcount[r] = (hi - lo) - hl;
-      atomicMax(&blk_maxnnz[r / kBlockRows], (int32_t)(hi - lo));
-    }
-  }
-}
-
-// head32[b][c][rr] = value of feature c (< p) of row 128*b + rr
-__global__ void k_head32_scatter(const int64_t* __restrict__ rp2, const int32_t* __restrict__ col2,
-                                 const float* __restrict__ val2, const int32_t* __restrict__ hlen,
-                                 int64_t n, int p, float* __restrict__ head32) {
-  const int lane = threadIdx.x & 31;
-  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
-  for (int64_t r = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; r < n; r += warps) {
-    const int64_t lo = rp2[r];
-    const int64_t b = r / kBlockRows, rr = r % kBlockRows;
-    for (int64_t e = lo + lane; e < lo + hlen[r]; e += 32)
-      head32[(b * p + col2[e]) * kBlockRows + rr] = val2[e];
-  }
-}
-
-// BF16 head block, one 16 KB tile per (row block, 64-feature chunk): row rr
-// of the tile occupies bytes [128 rr, 128 rr + 128) and its 16-byte chunk c
-// (features 8c..8c+7 of the chunk) sits at chunk position c ^ (rr % 8), the
-// 128-byte swizzle the tensor core expects, so a plain bulk copy lands a tile
-// in shared memory ready for tcgen05.mma.
-__global__ void k_head16_scatter(const int64_t* __restrict__ rp2, const int32_t* __restrict__ col2,
-                                 const float* __restrict__ val2, const int32_t* __restrict__ hlen,
-                                 int64_t n, int nkc, __nv_bfloat16* __restrict__ head16) {
-  const int lane = threadIdx.x & 31;
-  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
-  for (int64_t r = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; r < n; r += warps) {
-    const int64_t lo = rp2[r];
-    const int64_t b = r / kBlockRows, rr = r % kBlockRows;
-    for (int64_t e = lo + lane; e < lo + hlen[r]; e += 32) {
-      const int f = col2[e];
-      const int kc = f >> 6, c = (f >> 3) & 7, w = f & 7;
-      const int64_t off = (((b * nkc + kc) * kBlockRows + rr) * 128 + ((c ^ (int)(rr & 7)) * 16)) / 2 + w;
-      head16[off] = __float2bfloat16_rn(val2[e]);
+      hlen[i] = (int32_t)nh;
+      nnz_row[i] = (int32_t)(hi - lo);
+      hnorm[i] = __double2float_ru(sqrt(hs));
+      tcount[i] = nt;
+      atomicMax(&blk_maxnnz[b], (int32_t)(hi - lo));
     }
   }
 }
@@ -302,7 +264,7 @@ __device__ __forceinline__ uint32_t tail_unrot(uint32_t k, int fb) {
 // One warp per new row: tail entries in row order (entry -> CSR index,
 // row in block, value, tail feature), posting counts per tail feature and,
 // when given, radix sort keys for the block-local lists (block, bucket,
-// tag), the half-block lists (half-block, feature) and the global lists
+// tag), the J-segment lists (J segment, feature) and the global lists
 // (feature, row).
 __global__ void k_tail_entries(const int64_t* __restrict__ rp2, const int32_t* __restrict__ col2,
                                const float* __restrict__ val2, const int32_t* __restrict__ hlen,
@@ -319,7 +281,7 @@ __global__ void k_tail_entries(const int64_t* __restrict__ rp2, const int32_t* _
     const int64_t lo = rp2[r] + hlen[r], hi = rp2[r + 1];
     const int64_t t0 = tptr[r];
     const uint64_t blk = (uint64_t)(r / kBlockRows);
-    const uint64_t hblk = (uint64_t)(r / (kBlockRows / 2));
+    const uint64_t hblk = (uint64_t)(r / kJSegRows);
     for (int64_t k = lo + lane; k < hi; k += 32) {
       const int64_t t = t0 + (k - lo);
       const int32_t f = col2[k] - p;
@@ -368,7 +330,7 @@ __global__ void k_bil_fill(const uint64_t* __restrict__ keys, const uint32_t* __
   }
 }
 
-// Packed J-side postings in (half-block, feature, row) order.
+// Packed J-side postings in (J segment, feature, row) order.
 __global__ void k_rec_fill(const uint64_t* __restrict__ keys, const uint32_t* __restrict__ vals,
                            const uint8_t* __restrict__ tr, const float* __restrict__ tu, int64_t T,
                            uint64_t fmask, uint2* __restrict__ rec) {
@@ -381,132 +343,136 @@ __global__ void k_rec_fill(const uint64_t* __restrict__ keys, const uint32_t* __
 }
 
 // ---- per-segment sorts in shared memory ----
-// The block-local lists and the half-block lists are orders of contiguous
-// row-order segments (an I block's tail entries, a half-block's) by keys
+// The block-local lists and the J-segment lists are orders of contiguous
+// row-order segments (an I block's tail entries, a J segment's) by keys
 // that are unique inside the segment (a feature occurs once per row), so the
 // sorted order is unique: one CTA sorts a segment in shared memory with a
-// bitonic network over the next power of two (padded with 0xffffffff keys)
-// and writes the postings directly. The result equals the stable global
-// radix sort by (segment, key) that is used when a segment exceeds
-// kSegMax entries.
-constexpr int kSegMax = 16384;   // entries per segment sorted in shared memory (128 KB)
-constexpr int kSegThreads = 512;
+// stable LSD radix sort and writes the postings directly. The result equals
+// the stable global radix sort by (segment, key) that is used when a segment
+// exceeds kSegMax entries.
+constexpr int kSegMax = 16384;   // entries per segment sorted in shared memory
+constexpr int kSegThreads = 1024;
 // Size classes of the segments: shared-memory capacity (entries) and threads
 // per CTA, so that small segments run many CTAs per SM.
 constexpr int kSegClasses = 3;
 constexpr int kSegCap[kSegClasses] = {1024, 4096, kSegMax};
 constexpr int kSegThr[kSegClasses] = {128, 256, kSegThreads};
+constexpr int kSegBins = 512;    // digits of up to 9 bits
 
-// One compare-exchange step of distance j < 32 on a 64-element chunk held
-// by a warp: lane l holds positions c0 + l (x0) and c0 + 32 + l (x1).
-__device__ __forceinline__ void seg_shfl_step(uint32_t& x, uint32_t& v, int pos, int j, int k) {
-  const uint32_t y = __shfl_xor_sync(0xffffffffu, x, j);
-  const uint32_t w = __shfl_xor_sync(0xffffffffu, v, j);
-  const bool up = ((pos & ~j) & k) == 0;  // direction of the pair (its lower position)
-  const bool lower = (pos & j) == 0;
-  // the lower position keeps the smaller key when ascending, the larger otherwise
-  const bool take = (lower == up) ? (y < x) : (y > x);
-  if (take) {
-    x = y;
-    v = w;
-  }
+// Shared memory of a segment sort with NT threads and cap entries:
+// keys K[cap], values V[cap], per-warp digit counters [NT/32][kSegBins],
+// digit starts [kSegBins].
+constexpr size_t seg_smem_bytes(int nt, int cap) {
+  return (size_t)cap * 8 + (size_t)(nt / 32) * kSegBins * 4 + (size_t)kSegBins * 4;
 }
 
-// Steps j = jmax .. 1 of stages k = kfirst .. klast (powers of two, each
-// stage starting at min(k / 2, jmax)) on the 64-element chunks, in
-// registers: j = 32 pairs a lane's two elements, j < 32 pairs lanes.
-__device__ __forceinline__ void seg_chunk_steps(uint32_t* K, uint32_t* V, int n2, int kfirst,
-                                                int klast, int jmax) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  for (int c0 = warp * 64; c0 < n2; c0 += nw * 64) {
-    const int p0 = c0 + lane, p1 = p0 + 32;
-    uint32_t x0 = K[p0], x1 = K[p1], v0 = V[p0], v1 = V[p1];
-    for (int k = kfirst; k <= klast; k <<= 1) {
-      for (int j = min(k >> 1, jmax); j > 0; j >>= 1) {
-        if (j == 32) {
-          if ((x0 > x1) == ((p0 & k) == 0)) {
-            const uint32_t tx = x0, tv = v0;
-            x0 = x1;
-            v0 = v1;
-            x1 = tx;
-            v1 = tv;
-          }
-        } else {
-          seg_shfl_step(x0, v0, p0, j, k);
-          seg_shfl_step(x1, v1, p1, j, k);
+// Stable LSD radix sort of (K, V)[0, len) by key bits [0, bits), len <= NT * E,
+// in passes of equal digits of at most 9 bits. Between passes the elements
+// live in registers: warp w holds positions [32 E w, 32 E (w + 1)) in chunks
+// of 32 lanes (position order = the order so far), ranks each chunk's digits
+// with match_any against per-warp counters, and the block scatters through
+// the one shared buffer: digit start + the count of that digit in earlier
+// warps + earlier in this warp.
+template <int NT, int E>
+__device__ __forceinline__ void seg_radix_sort(uint32_t* K, uint32_t* V, uint32_t* wcnt,
+                                               uint32_t* dstart, int len, int bits) {
+  constexpr int NW = NT / 32;
+  constexpr int BPT = kSegBins / NT > 0 ? kSegBins / NT : 1;  // digits per thread (max)
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const unsigned lt = (1u << lane) - 1u;
+  const int passes = bits <= 0 ? 0 : (bits + 8) / 9;
+  const int rb = passes ? (bits + passes - 1) / passes : 0;
+  const int bins = 1 << rb;
+  const uint32_t dmask = (uint32_t)bins - 1u;
+  const int bpt = (bins + NT - 1) / NT;
+  static_assert(E % 2 == 0 && NT * E <= 65536, "ranks are packed two per register");
+  uint32_t key[E], val[E], rank2[E / 2];  // rank of chunk c in bits 16 (c & 1) of rank2[c / 2]
+  for (int pass = 0, shift = 0; pass < passes; ++pass, shift += rb) {
+    for (int i = threadIdx.x; i < NW * kSegBins; i += NT) wcnt[i] = 0;
+#pragma unroll
+    for (int c = 0; c < E; ++c) {
+      const int idx = w * 32 * E + c * 32 + lane;
+      const bool valid = idx < len;
+      key[c] = valid ? K[idx] : 0u;
+      val[c] = valid ? V[idx] : 0u;
+    }
+    __syncthreads();
+    uint32_t* mine = wcnt + w * kSegBins;
+#pragma unroll
+    for (int c = 0; c < E; ++c) {
+      const bool valid = w * 32 * E + c * 32 + lane < len;
+      const unsigned vmask = __ballot_sync(0xffffffffu, valid);
+      uint32_t before = 0, peers = 0;
+      const uint32_t d = (key[c] >> shift) & dmask;
+      if (valid) {
+        peers = __match_any_sync(vmask, d);
+        before = mine[d];
+      }
+      __syncwarp();
+      if (valid && lane == __ffs(peers) - 1) mine[d] = before + __popc(peers);
+      __syncwarp();
+      const uint32_t r = before + __popc(peers & lt);
+      if (c & 1) rank2[c / 2] |= r << 16;
+      else rank2[c / 2] = r;
+    }
+    __syncthreads();
+    // per digit: each warp's offset inside the digit, the digit's total;
+    // then the exclusive scan of the totals over digits
+    uint32_t dtot[BPT];
+    uint32_t tsum = 0;
+#pragma unroll
+    for (int k = 0; k < BPT; ++k) {
+      const int d = threadIdx.x * bpt + k;
+      uint32_t run = 0;
+      if (k < bpt && d < bins) {
+        for (int ww = 0; ww < NW; ++ww) {
+          const uint32_t t = wcnt[ww * kSegBins + d];
+          wcnt[ww * kSegBins + d] = run;
+          run += t;
         }
       }
+      dtot[k] = run;
+      tsum += run;
     }
-    K[p0] = x0;
-    K[p1] = x1;
-    V[p0] = v0;
-    V[p1] = v1;
-  }
-}
-
-// Bitonic sort of n2 (a power of two) key/value pairs in shared memory:
-// steps of distance >= 64 exchange through shared memory, the others run in
-// registers on 64-element chunks (one warp per chunk).
-__device__ __forceinline__ void seg_bitonic(uint32_t* K, uint32_t* V, int n2) {
-  if (n2 < 64) {
-    for (int k = 2; k <= n2; k <<= 1) {
-      for (int j = k >> 1; j > 0; j >>= 1) {
-        for (int i = threadIdx.x; i < (n2 >> 1); i += blockDim.x) {
-          const int lo = ((i & ~(j - 1)) << 1) | (i & (j - 1));
-          const int hi = lo + j;
-          const uint32_t a = K[lo], b = K[hi];
-          if ((a > b) == ((lo & k) == 0)) {
-            K[lo] = b;
-            K[hi] = a;
-            const uint32_t va = V[lo];
-            V[lo] = V[hi];
-            V[hi] = va;
-          }
-        }
-        __syncthreads();
+    uint32_t total;
+    uint32_t start = block_excl_scan<uint32_t, NT>(tsum, &total);
+#pragma unroll
+    for (int k = 0; k < BPT; ++k) {
+      const int d = threadIdx.x * bpt + k;
+      if (k < bpt && d < bins) {
+        dstart[d] = start;
+        start += dtot[k];
       }
     }
-    return;
-  }
-  seg_chunk_steps(K, V, n2, 2, 64, 32);  // stages 2 .. 64: inside the chunks
-  __syncthreads();
-  for (int k = 128; k <= n2; k <<= 1) {
-    for (int j = k >> 1; j >= 64; j >>= 1) {
-      for (int i = threadIdx.x; i < (n2 >> 1); i += blockDim.x) {
-        const int lo = ((i & ~(j - 1)) << 1) | (i & (j - 1));
-        const int hi = lo + j;
-        const uint32_t a = K[lo], b = K[hi];
-        if ((a > b) == ((lo & k) == 0)) {
-          K[lo] = b;
-          K[hi] = a;
-          const uint32_t va = V[lo];
-          V[lo] = V[hi];
-          V[hi] = va;
-        }
+    __syncthreads();
+#pragma unroll
+    for (int c = 0; c < E; ++c) {
+      if (w * 32 * E + c * 32 + lane < len) {
+        const uint32_t d = (key[c] >> shift) & dmask;
+        const uint32_t pos = dstart[d] + mine[d] + ((rank2[c / 2] >> (16 * (c & 1))) & 0xffffu);
+        K[pos] = key[c];
+        V[pos] = val[c];
       }
-      __syncthreads();
     }
-    seg_chunk_steps(K, V, n2, k, k, 32);
     __syncthreads();
   }
 }
 
-// Loads the segment [s0, s0 + len) as (key(t), value bits) pairs, padded to
-// n2, and sorts it.
-template <typename KeyOf>
-__device__ __forceinline__ void seg_load_sort(uint32_t* K, uint32_t* V, int64_t s0, int len,
-                                              int n2, const float* __restrict__ tu, KeyOf key) {
-  for (int i = threadIdx.x; i < n2; i += blockDim.x) {
-    if (i < len) {
-      K[i] = key(s0 + i);
-      V[i] = __float_as_uint(tu[s0 + i]);
-    } else {
-      K[i] = 0xffffffffu;
-      V[i] = 0u;
-    }
+// Loads the segment [s0, s0 + len) as (key(t), value bits) pairs and sorts
+// it by the low `bits` bits of the keys.
+template <int NT, int E, typename KeyOf>
+__device__ __forceinline__ void seg_load_sort(uint32_t* smem, int cap, int64_t s0, int len,
+                                              int bits, const float* __restrict__ tu, KeyOf key) {
+  uint32_t* K = smem;
+  uint32_t* V = smem + cap;
+  uint32_t* wcnt = smem + 2 * cap;
+  uint32_t* dstart = wcnt + (NT / 32) * kSegBins;
+  for (int i = threadIdx.x; i < len; i += NT) {
+    K[i] = key(s0 + i);
+    V[i] = __float_as_uint(tu[s0 + i]);
   }
   __syncthreads();
-  seg_bitonic(K, V, n2);
+  seg_radix_sort<NT, E>(K, V, wcnt, dstart, len, bits);
 }
 
 // Non-empty segments of ptr (nseg segments, host copy) grouped by size
@@ -532,34 +498,29 @@ inline cuapss_status seg_classes(const std::vector<int64_t>& ptr, int nseg, Work
   return CUAPSS_OK;
 }
 
-__device__ __forceinline__ int seg_pow2(int len) {
-  int n2 = 2;
-  while (n2 < len) n2 <<= 1;
-  return n2;
-}
-
 // I-side postings of one 128-row block (one CTA per block of the list
 // ids): sort key {rotated feature << 7 | row in block}; writes bil_key,
 // bil_u, bil_len in the layout of k_bil_fill.
-__global__ void __launch_bounds__(kSegThreads) k_bil_seg(const int32_t* __restrict__ ids,
-                                                         const int64_t* __restrict__ bptr,
-                                                         const uint32_t* __restrict__ tf,
-                                                         const uint8_t* __restrict__ tr,
-                                                         const float* __restrict__ tu, int fb,
-                                                         uint32_t* __restrict__ bil_key,
-                                                         float* __restrict__ bil_u,
-                                                         uint8_t* __restrict__ bil_len, int cap) {
+template <int NT, int E>
+__global__ void __launch_bounds__(NT) k_bil_seg(const int32_t* __restrict__ ids,
+                                                const int64_t* __restrict__ bptr,
+                                                const uint32_t* __restrict__ tf,
+                                                const uint8_t* __restrict__ tr,
+                                                const float* __restrict__ tu, int fb,
+                                                uint32_t* __restrict__ bil_key,
+                                                float* __restrict__ bil_u,
+                                                uint8_t* __restrict__ bil_len) {
   extern __shared__ uint32_t seg_sm[];
-  uint32_t* K = seg_sm;
-  uint32_t* V = seg_sm + cap;
+  constexpr int cap = NT * E;
+  const uint32_t* K = seg_sm;
+  const uint32_t* V = seg_sm + cap;
   const int b = ids[blockIdx.x];
   const int64_t s0 = bptr[b];
   const int len = (int)(bptr[b + 1] - s0);
   if (len <= 0) return;
-  const int n2 = seg_pow2(len);
-  seg_load_sort(K, V, s0, len, n2, tu,
-                [&](int64_t t) { return (tail_rot(tf[t], fb) << 7) | (uint32_t)tr[t]; });
-  for (int i = threadIdx.x; i < len; i += blockDim.x) {
+  seg_load_sort<NT, E>(seg_sm, cap, s0, len, fb + 7, tu,
+                       [&](int64_t t) { return (tail_rot(tf[t], fb) << 7) | (uint32_t)tr[t]; });
+  for (int i = threadIdx.x; i < len; i += NT) {
     const uint32_t k = K[i], rf = k >> 7;
     const uint32_t f = tail_unrot(rf, fb);
     bil_key[s0 + i] =
@@ -575,37 +536,39 @@ __global__ void __launch_bounds__(kSegThreads) k_bil_seg(const int32_t* __restri
   }
 }
 
-// J-side postings of one 64-row half-block (one CTA per half-block of the
-// list ids): sort key {feature << 6 | row in half}; writes records in the
+// J-side postings of one kJSegRows-row segment (one CTA per segment of the
+// list ids): sort key {feature << 5 | row in segment}; writes records in the
 // layout of k_rec_fill.
-__global__ void __launch_bounds__(kSegThreads) k_rec_seg(const int32_t* __restrict__ ids,
-                                                         const int64_t* __restrict__ hptr,
-                                                         const uint32_t* __restrict__ tf,
-                                                         const uint8_t* __restrict__ tr,
-                                                         const float* __restrict__ tu,
-                                                         uint2* __restrict__ rec, int cap) {
+template <int NT, int E>
+__global__ void __launch_bounds__(NT) k_rec_seg(const int32_t* __restrict__ ids,
+                                                const int64_t* __restrict__ hptr,
+                                                const uint32_t* __restrict__ tf,
+                                                const uint8_t* __restrict__ tr,
+                                                const float* __restrict__ tu, int fb,
+                                                uint2* __restrict__ rec) {
   extern __shared__ uint32_t seg_sm[];
-  uint32_t* K = seg_sm;
-  uint32_t* V = seg_sm + cap;
+  constexpr int cap = NT * E;
+  const uint32_t* K = seg_sm;
+  const uint32_t* V = seg_sm + cap;
   const int h = ids[blockIdx.x];
   const int64_t s0 = hptr[h];
   const int len = (int)(hptr[h + 1] - s0);
   if (len <= 0) return;
-  const int n2 = seg_pow2(len);
-  seg_load_sort(K, V, s0, len, n2, tu,
-                [&](int64_t t) { return (tf[t] << 6) | ((uint32_t)tr[t] & 63u); });
-  const uint32_t half = (uint32_t)(h & 1) << 6;
-  for (int i = threadIdx.x; i < len; i += blockDim.x) {
+  static_assert(kJSegRows == 32, "row in segment: 5 bits");
+  seg_load_sort<NT, E>(seg_sm, cap, s0, len, fb + 5, tu,
+                       [&](int64_t t) { return (tf[t] << 5) | ((uint32_t)tr[t] & 31u); });
+  const uint32_t seg0 = (uint32_t)(h % kJSegs) * kJSegRows;  // first block row of the segment
+  for (int i = threadIdx.x; i < len; i += NT) {
     const uint32_t k = K[i];
-    rec[s0 + i] = make_uint2(((k >> 6) << 8) | half | (k & 63u), V[i]);
+    rec[s0 + i] = make_uint2(((k >> 5) << 8) | seg0 | (k & 31u), V[i]);
   }
 }
 
-__global__ void k_half_ptrs(const int64_t* __restrict__ tptr, int64_t n, int nh,
-                            int64_t* __restrict__ hptr) {
+__global__ void k_seg_ptrs(const int64_t* __restrict__ tptr, int64_t n, int nh,
+                           int64_t* __restrict__ hptr) {
   for (int64_t h = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; h <= nh;
        h += (int64_t)gridDim.x * blockDim.x)
-    hptr[h] = tptr[min(n, h * (kBlockRows / 2))];
+    hptr[h] = tptr[min(n, (int64_t)h * kJSegRows)];
 }
 
 __global__ void k_block_ptrs(const int64_t* __restrict__ tptr, int64_t n, int nb,
@@ -654,6 +617,46 @@ inline unsigned grid_for(int64_t work, int per_block) {
   return (unsigned)std::min<int64_t>(g, 148 * 32);
 }
 
+// Kernel attributes of the segment sorts (their shared memory), once per
+// device.
+cuapss_status seg_sort_init() {
+  static std::mutex mu;
+  static uint64_t done = 0;  // bit per device
+  int dev = 0;
+  CU_TRY(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lk(mu);
+  if (dev < 64 && ((done >> dev) & 1ull)) return CUAPSS_OK;
+  constexpr int C = kSegClasses - 1;
+  constexpr int NT = kSegThr[C], E = kSegCap[C] / kSegThr[C];
+  const int sm = (int)seg_smem_bytes(NT, kSegCap[C]);
+  CU_TRY(cudaFuncSetAttribute(k_bil_seg<NT, E>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+  CU_TRY(cudaFuncSetAttribute(k_rec_seg<NT, E>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+  if (dev < 64) done |= 1ull << dev;
+  return CUAPSS_OK;
+}
+
+// Segment sorts of size class C: the I blocks' lists and the J segments'
+// records whose lengths fall in the class.
+template <int C>
+cuapss_status launch_seg_sorts(const int32_t* idsB, const int (&fB)[kSegClasses + 1],
+                               const int32_t* idsH, const int (&fH)[kSegClasses + 1], Side& s,
+                               const uint32_t* tf, int fb, cudaStream_t st) {
+  constexpr int NT = kSegThr[C], E = kSegCap[C] / kSegThr[C];
+  static_assert(NT * E == kSegCap[C], "class capacity");
+  const size_t sm = seg_smem_bytes(NT, kSegCap[C]);
+  if (fB[C + 1] > fB[C]) {
+    k_bil_seg<NT, E><<<fB[C + 1] - fB[C], NT, sm, st>>>(idsB + fB[C], s.bptr, tf, s.tr, s.tu, fb,
+                                                       s.bil_key, s.bil_u, s.bil_len);
+    LAUNCH_CHECK();
+  }
+  if (fH[C + 1] > fH[C]) {
+    k_rec_seg<NT, E><<<fH[C + 1] - fH[C], NT, sm, st>>>(idsH + fH[C], s.hptr, tf, s.tr, s.tu, fb,
+                                                       s.bil_rec);
+    LAUNCH_CHECK();
+  }
+  return CUAPSS_OK;
+}
+
 }  // namespace
 
 cuapss_status validate_csr(const int64_t* rp, const int32_t* col, const float* val, int64_t n,
@@ -672,27 +675,39 @@ cuapss_status validate_csr(const int64_t* rp, const int32_t* col, const float* v
   CU_TRY(cudaMemcpyAsync(&h_err, err, sizeof(int), cudaMemcpyDeviceToHost, st));
   CU_TRY(cudaStreamSynchronize(st));
   if (h_err) return CUAPSS_EINVAL;
-  if (counts && d <= kHistMax && nnz >= 4 * d) {
+  const int mode = !counts ? kHistGlobal
+                   : (d <= kHistMax && nnz >= 4 * d) ? kHistDirect
+                   : (d > kHistMax && nnz >= ((int64_t)1 << 22)) ? kHistHashed
+                                                                  : kHistGlobal;
+  if (mode != kHistGlobal) {
     static std::mutex mu;
-    static uint64_t done = 0;  // attribute set, bit per device
+    static uint64_t done = 0;  // attributes set, bit per device
     int dev = 0;
     CU_TRY(cudaGetDevice(&dev));
     {
       std::lock_guard<std::mutex> lk(mu);
       if (dev >= 64 || !((done >> dev) & 1ull)) {
-        CU_TRY(cudaFuncSetAttribute(k_check_rows<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        CU_TRY(cudaFuncSetAttribute(k_check_rows<kHistDirect>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)(kHistMax * sizeof(int))));
+        CU_TRY(cudaFuncSetAttribute(k_check_rows<kHistHashed>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)(2 * kHashSlots * sizeof(int))));
         if (dev < 64) done |= 1ull << dev;
       }
     }
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const unsigned g = (unsigned)std::max<int64_t>(1, std::min<int64_t>(sms, ceil_div(n, 32)));
-    k_check_rows<true><<<g, 1024, (size_t)d * sizeof(int), st>>>(rp, col, val, n, d, tol, check,
-                                                                  counts, err, nm);
+    if (mode == kHistDirect)
+      k_check_rows<kHistDirect><<<g, 1024, (size_t)d * sizeof(int), st>>>(
+          rp, col, val, n, d, tol, check, counts, err, nm);
+    else
+      k_check_rows<kHistHashed><<<g, 1024, 2 * kHashSlots * sizeof(int), st>>>(
+          rp, col, val, n, d, tol, check, counts, err, nm);
   } else {
-    k_check_rows<false><<<grid_for(n * 32, kThreads), kThreads, 0, st>>>(rp, col, val, n, d, tol,
-                                                                       check, counts, err, nm);
+    k_check_rows<kHistGlobal><<<grid_for(n * 32, kThreads), kThreads, 0, st>>>(
+        rp, col, val, n, d, tol, check, counts, err, nm);
   }
   LAUNCH_CHECK();
   unsigned long long h_nm = 0;
@@ -742,47 +757,15 @@ cuapss_status build_side(Side& s, const PrepOptions& o, const int32_t* perm, Wor
   const uint64_t fmask = (fbits >= 64) ? ~0ull : ((1ull << fbits) - 1);
   const uint64_t rmask = (1ull << rbits) - 1;
   const std::string t = tag + ":";
-  // ---- row order (nnz descending, then id) ----
-  int32_t* rowinv = nullptr;
-  int64_t* newlen = nullptr;
-  uint64_t* rkeys = nullptr;
-  uint32_t* rvals = nullptr;
+  // ---- rows keep the caller's order: identity row map, rp2 = rp0 ----
   ST_TRY(ws.get(t + "rowperm", (size_t)n, &s.rowperm));
-  ST_TRY(ws.get(t + "rowinv", (size_t)n, &rowinv));
-  ST_TRY(ws.get(t + "newlen", (size_t)n + 1, &newlen));
-  ST_TRY(ws.get(t + "rkeys", (size_t)n, &rkeys));
-  ST_TRY(ws.get(t + "rvals", (size_t)n, &rvals));
-  k_row_keys<<<grid_for(n, kThreads), kThreads, 0, st>>>(s.rp0, n, d, rbits, rkeys, rvals);
-  LAUNCH_CHECK();
-  if (o.row_sort)
-    ST_TRY(radix_sort_pairs(rkeys, rvals, n, rbits + fbits + 1, ws, t + "rows", st));
-  k_rowperm<<<grid_for(n, kThreads), kThreads, 0, st>>>(rvals, s.rp0, n, s.rowperm, rowinv, newlen);
+  k_iota_i32<<<grid_for(n, kThreads), kThreads, 0, st>>>(s.rowperm, n);
   LAUNCH_CHECK();
   ST_TRY(ws.get(t + "rp2", (size_t)n + 1, &s.rp2));
-  ST_TRY(exclusive_scan<int64_t>(newlen, s.rp2, n, s.rp2 + n, ws, t + "rp2", st));
-  // ---- remapped CSR: each row's head entries (rank < p) first ----
-  ST_TRY(ws.get(t + "col2", (size_t)nnz, &s.col2));
-  ST_TRY(ws.get(t + "val2", (size_t)nnz, &s.val2));
-  if (!o.row_sort) {
-    // rows keep their place (rp2 == rp0): split each row in one pass
-    k_split_rows<<<grid_for(n * 32, kThreads), kThreads, 0, st>>>(s.rp0, s.col0, s.val0, perm, n,
-                                                                  p, s.col2, s.val2);
-    LAUNCH_CHECK();
-  } else {
-    // rows reordered: one radix sort of all entries on (new row, rank)
-    uint64_t* ekeys = nullptr;
-    uint32_t* evals = nullptr;
-    ST_TRY(ws.get(t + "ekeys", (size_t)nnz, &ekeys));
-    ST_TRY(ws.get(t + "evals", (size_t)nnz, &evals));
-    k_entry_keys<<<grid_for(n * 32, kThreads), kThreads, 0, st>>>(s.rp0, s.col0, perm, rowinv, n,
-                                                                  fbits, ekeys, evals);
-    LAUNCH_CHECK();
-    ST_TRY(radix_sort_pairs(ekeys, evals, nnz, rbits + fbits, ws, t + "ent", st));
-    k_gather_entries<<<grid_for(nnz, kThreads), kThreads, 0, st>>>(ekeys, evals, s.val0, nnz,
-                                                                   fmask, s.col2, s.val2);
-    LAUNCH_CHECK();
-  }
-  // ---- per-row statistics ----
+  CU_TRY(cudaMemcpyAsync(s.rp2, s.rp0, sizeof(int64_t) * (n + 1), cudaMemcpyDeviceToDevice, st));
+  // ---- one pass: remap, head block, row statistics, tail suffixes ----
+  ST_TRY(ws.get(t + "col2", (size_t)std::max<int64_t>(nnz, 1), &s.col2));
+  ST_TRY(ws.get(t + "val2", (size_t)std::max<int64_t>(nnz, 1), &s.val2));
   int64_t* tcount = nullptr;
   ST_TRY(ws.get(t + "hlen", (size_t)n, &s.hlen));
   ST_TRY(ws.get(t + "nnzrow", (size_t)n, &s.nnz_row));
@@ -790,39 +773,34 @@ cuapss_status build_side(Side& s, const PrepOptions& o, const int32_t* perm, Wor
   ST_TRY(ws.get(t + "tcount", (size_t)n + 1, &tcount));
   ST_TRY(ws.get(t + "blkmax", (size_t)nb + 1, &s.blk_maxnnz));
   CU_TRY(cudaMemsetAsync(s.blk_maxnnz, 0, sizeof(int32_t) * (nb + 1), st));
-  k_row_stats<<<grid_for(n * 32, kThreads), kThreads, 0, st>>>(s.rp2, s.col2, s.val2, n, p, s.hlen,
-                                                               s.nnz_row, s.hnorm, tcount,
-                                                               s.blk_maxnnz);
-  LAUNCH_CHECK();
-  ST_TRY(ws.get(t + "tptr", (size_t)n + 1, &s.tptr));
-  ST_TRY(exclusive_scan<int64_t>(tcount, s.tptr, n, s.tptr + n, ws, t + "tptr", st));
-  // ---- dense FP32 head block ----
+  s.head32 = nullptr;
+  s.head16 = nullptr;
+  int nkc = 0;
   if (o.want_head32 && p > 0) {
     const size_t hb = (size_t)nb * p * kBlockRows;
     ST_TRY(ws.get(t + "head32", hb, &s.head32));
     CU_TRY(cudaMemsetAsync(s.head32, 0, hb * sizeof(float), st));
-    k_head32_scatter<<<grid_for(n * 32, kThreads), kThreads, 0, st>>>(s.rp2, s.col2, s.val2,
-                                                                      s.hlen, n, p, s.head32);
-    LAUNCH_CHECK();
   }
-  // ---- dense BF16 head block (tensor-core path) ----
   if (o.want_head16 && p > 0) {
     if (p % 64 != 0) return CUAPSS_EINVAL;
-    const int nkc = p / 64;
+    nkc = p / 64;
     const size_t hb = (size_t)nb * nkc * kBlockRows * 64;
     ST_TRY(ws.get(t + "head16", hb, &s.head16));
     CU_TRY(cudaMemsetAsync(s.head16, 0, hb * sizeof(__nv_bfloat16), st));
-    k_head16_scatter<<<grid_for(n * 32, kThreads), kThreads, 0, st>>>(s.rp2, s.col2, s.val2,
-                                                                      s.hlen, n, nkc, s.head16);
-    LAUNCH_CHECK();
   }
-  // ---- tail: segment pointers (blocks, half-blocks), host copies ----
-  const int nh = 2 * nb;  // half-blocks, the last one possibly empty
+  k_split_rows<<<grid_for(n * 32, kThreads), kThreads, 0, st>>>(
+      s.rp0, s.col0, s.val0, perm, n, p, s.col2, s.val2, s.hlen, s.nnz_row, s.hnorm, tcount,
+      s.blk_maxnnz, s.head16, nkc, s.head32);
+  LAUNCH_CHECK();
+  ST_TRY(ws.get(t + "tptr", (size_t)n + 1, &s.tptr));
+  ST_TRY(exclusive_scan<int64_t>(tcount, s.tptr, n, s.tptr + n, ws, t + "tptr", st));
+  // ---- tail: segment pointers (blocks, J segments), host copies ----
+  const int nh = kJSegs * nb;  // J segments, the last ones possibly empty
   ST_TRY(ws.get(t + "bptr", (size_t)nb + 1, &s.bptr));
   ST_TRY(ws.get(t + "hptr", (size_t)nh + 1, &s.hptr));
   k_block_ptrs<<<grid_for(nb + 1, kThreads), kThreads, 0, st>>>(s.tptr, n, nb, s.bptr);
   LAUNCH_CHECK();
-  k_half_ptrs<<<grid_for(nh + 1, kThreads), kThreads, 0, st>>>(s.tptr, n, nh, s.hptr);
+  k_seg_ptrs<<<grid_for(nh + 1, kThreads), kThreads, 0, st>>>(s.tptr, n, nh, s.hptr);
   LAUNCH_CHECK();
   std::vector<int64_t> h_hptr((size_t)nh + 1);
   s.h_bptr.resize(nb + 1);
@@ -874,31 +852,17 @@ cuapss_status build_side(Side& s, const PrepOptions& o, const int32_t* perm, Wor
   ST_TRY(ws.get(t + "bil_len", (size_t)T, &s.bil_len));
   ST_TRY(ws.get(t + "bil_rec", (size_t)T, &s.bil_rec));
   if (seg_sort) {
-    // block-local lists in (bucket, tag, row) order and half-block records in
+    // block-local lists in (bucket, tag, row) order and J-segment records in
     // (feature, row) order, one CTA per segment
     if (T > 0) {
-      CU_TRY(cudaFuncSetAttribute(k_bil_seg, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)(2 * sizeof(uint32_t) * kSegMax)));
-      CU_TRY(cudaFuncSetAttribute(k_rec_seg, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)(2 * sizeof(uint32_t) * kSegMax)));
+      ST_TRY(seg_sort_init());
       int32_t *idsB = nullptr, *idsH = nullptr;
       int fB[kSegClasses + 1], fH[kSegClasses + 1];
       ST_TRY(seg_classes(s.h_bptr, nb, ws, t + "segB", st, &idsB, fB));
       ST_TRY(seg_classes(h_hptr, nh, ws, t + "segH", st, &idsH, fH));
-      for (int c = 0; c < kSegClasses; ++c) {
-        const size_t sm = 2 * sizeof(uint32_t) * kSegCap[c];
-        if (fB[c + 1] > fB[c]) {
-          k_bil_seg<<<fB[c + 1] - fB[c], kSegThr[c], sm, st>>>(idsB + fB[c], s.bptr, tf, s.tr,
-                                                               s.tu, fb, s.bil_key, s.bil_u,
-                                                               s.bil_len, kSegCap[c]);
-          LAUNCH_CHECK();
-        }
-        if (fH[c + 1] > fH[c]) {
-          k_rec_seg<<<fH[c + 1] - fH[c], kSegThr[c], sm, st>>>(idsH + fH[c], s.hptr, tf, s.tr,
-                                                               s.tu, s.bil_rec, kSegCap[c]);
-          LAUNCH_CHECK();
-        }
-      }
+      ST_TRY(launch_seg_sorts<0>(idsB, fB, idsH, fH, s, tf, fb, st));
+      ST_TRY(launch_seg_sorts<1>(idsB, fB, idsH, fH, s, tf, fb, st));
+      ST_TRY(launch_seg_sorts<2>(idsB, fB, idsH, fH, s, tf, fb, st));
     }
   } else {
     // block-local inverted lists: stable sort by (block, bucket, tag) keeps
@@ -907,7 +871,7 @@ cuapss_status build_side(Side& s, const PrepOptions& o, const int32_t* perm, Wor
     k_bil_fill<<<grid_for(T, kThreads), kThreads, 0, st>>>(bkeys, bvals, s.tr, s.tu, T, fb,
                                                           s.bil_key, s.bil_u, s.bil_len);
     LAUNCH_CHECK();
-    // J-side postings: per 64-row half-block, sorted by feature, packed
+    // J-side postings: per kJSegRows-row segment, sorted by feature, packed
     ST_TRY(radix_sort_pairs(hkeys, hvals, T, std::max(1, bits_for((uint64_t)nh)) + fb, ws,
                             t + "rec", st));
     k_rec_fill<<<grid_for(T, kThreads), kThreads, 0, st>>>(hkeys, hvals, s.tr, s.tu, T,

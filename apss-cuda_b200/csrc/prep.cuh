@@ -1,5 +1,5 @@
-// Preparation of one join operand: validation, frequency remap, row order,
-// head block and inverted lists.
+// Preparation of one join operand: validation, frequency remap, head block
+// and inverted lists (rows keep the caller's order).
 #pragma once
 
 #include <string>
@@ -11,7 +11,6 @@ namespace cuapss {
 
 struct PrepOptions {
   int p = 64;           // head width (multiple of 32 for the FP32 head block)
-  int row_sort = 1;     // order rows by nnz descending
   int want_head32 = 1;  // build the FP32 head block
   int want_head16 = 0;  // build the BF16 head block
   int want_csc = 0;     // build the global inverted lists (cptr/csc)

@@ -4,7 +4,7 @@
 //
 // Layout. The index is a list of immutable segments, each a block-aligned
 // run of index rows [row0, row0 + n) with its own CSR copy and its prepared
-// J side (dense head block, head norms, block nnz maxima, per-half-block tail
+// J side (dense head block, head norms, block nnz maxima, per-J-segment tail
 // postings). The frequency remap (and so the head features) is fixed when the
 // index is created; appended rows use it too. An append builds a segment for
 // the new rows only, then merges trailing segments whose sizes are within a
@@ -175,7 +175,6 @@ cuapss_status build_segment(cuapss_ctx* ctx, const cuapss_index* idx, const DevC
   ST_TRY(H.copy(x.val, (size_t)std::max<int64_t>(x.nnz, 1), &seg->val, st));
   PrepOptions po;
   po.p = idx->p;
-  po.row_sort = 0;
   po.want_head32 = idx->mixed ? 0 : 1;
   po.want_head16 = idx->mixed ? 1 : 0;
   Side S;
@@ -202,7 +201,7 @@ cuapss_status build_segment(cuapss_ctx* ctx, const cuapss_index* idx, const DevC
   } else {
     ST_TRY(H.copy(S.head32, (size_t)nb * S.p * kBlockRows, &seg->head32, st));
   }
-  ST_TRY(H.copy(S.hptr, (size_t)2 * nb + 1, &seg->hptr, st));
+  ST_TRY(H.copy(S.hptr, (size_t)kJSegs * nb + 1, &seg->hptr, st));
   ST_TRY(H.copy(S.bil_rec, (size_t)std::max<int64_t>(S.ntail, 1), &seg->rec, st));
   CU_TRY(cudaStreamSynchronize(st));
   *out = std::move(seg);
@@ -421,7 +420,6 @@ cuapss_status cuapss::index_query_rows(cuapss_ctx* ctx, const cuapss_index* idx,
   // ---- query side (I role)
   PrepOptions po;
   po.p = idx->p;
-  po.row_sort = 0;
   po.want_head32 = idx->mixed ? 0 : 1;
   po.want_head16 = idx->mixed ? 1 : 0;
   Side SQ;

@@ -1,15 +1,15 @@
 // Device-resident layout of one operand of a similarity join, after
-// validation, frequency remap, row ordering and the index build.
+// validation, frequency remap and the index build.
 //
 // HBM layout (n rows, d features, nnz non-zeros, p head width, nb = ceil(n/128)
 // row blocks of 128 rows, T tail non-zeros):
-//   rowperm   int32[n]        new row -> caller's row (rows ordered by nnz
-//                             descending, then id)
-//   rp2       int64[n+1]      CSR of the remapped, row-ordered matrix
-//   col2/val2 int32/f32[nnz]  feature ids remapped by frequency rank; each
-//                             row holds its head entries (rank < p) first, a
-//                             prefix of length hlen[r], then its tail entries
-//                             (ascending in each part when rows are reordered)
+//   rowperm   int32[n]        row -> caller's row (rows keep the caller's
+//                             order: the identity)
+//   rp2       int64[n+1]      copy of the caller's rowptr
+//   col2/val2 int32/f32[nnz]  the tail entries of each row (features of rank
+//                             >= p, remapped to their frequency rank), as a
+//                             suffix of the row's range of length
+//                             nnz - hlen[r]; the head prefix is not written
 //   head32    f32[nb][p][128] dense head block, k-major inside a row block so
 //                             that a 32-feature slice of a block is one
 //                             contiguous 16 KB run (one bulk TMA copy)
@@ -26,9 +26,10 @@
 //                             key {bucket << 15 | tag << 7 | row in block},
 //                             value, and the length of each feature's run at
 //                             its first posting
-//   bil_rec   uint2[T]        the same postings per 64-row half-block, sorted by
-//                             feature, packed {feature << 8 | row, value}
-//   hptr      int64[2nb+1]    postings of each half-block
+//   bil_rec   uint2[T]        the same postings per kJSegRows-row segment,
+//                             sorted by feature, packed {feature << 8 | row in
+//                             block, value}
+//   hptr      int64[kJSegs nb + 1]  postings of each J segment
 #pragma once
 
 #include <cuda_bf16.h>
@@ -68,9 +69,9 @@ struct Side {
   uint32_t* bil_key = nullptr;    // I-side postings {bucket << 15 | tag << 7 | row}
   float* bil_u = nullptr;
   uint8_t* bil_len = nullptr;     // run length at a feature's first posting, else 0
-  uint2* bil_rec = nullptr;       // J-side postings per 64-row half-block, sorted by
+  uint2* bil_rec = nullptr;       // J-side postings per kJSegRows-row segment, sorted by
                                   // feature: {feature << 8 | row in block, value bits}
-  int64_t* hptr = nullptr;        // [2 nb + 1] postings of each half-block
+  int64_t* hptr = nullptr;        // [kJSegs nb + 1] postings of each J segment
   int64_t ntail = 0;
   int64_t max_block_tail = 0;
   std::vector<int64_t> h_bptr;    // host copy of bptr (unit scheduling)

@@ -13,8 +13,9 @@
 // many postings (any cut is valid: every chunk adds the products
 // of its own postings; a run cut by a chunk boundary is re-measured).
 //
-// J side (the columns; one per tile): the tail postings of each 64-row
-// half-block sorted by feature, packed as {feature << 8 | column, value}.
+// J side (the columns; one per tile): the tail postings of each
+// kJSegRows-row segment of the J block sorted by feature, packed as
+// {feature << 8 | column, value}.
 // A J posting (c, f, v) reads the two offsets of bucket f mod 2^12 and walks
 // that bucket run by run (tags ascend) to the run with tag f >> 12; each of
 // its postings (r, u) adds u * v into the shared-memory accumulator

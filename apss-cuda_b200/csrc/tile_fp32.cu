@@ -114,7 +114,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_tiles_fp32(const TileArgs A) {
         // ---- tail: J's postings probe I's staged feature groups
         {
           int* acc = reinterpret_cast<int*>(S.acc);
-          const int64_t k0 = A.hptrJ[2 * J], k1 = A.hptrJ[2 * J + 2];
+          const int64_t k0 = A.hptrJ[kJSegs * J], k1 = A.hptrJ[kJSegs * (J + 1)];
           if (nch == 1) {
             tail_postings<8>(A, S.ts, T, k0, k1, acc, kAccLd, 0, tid, kThreads);
           } else {

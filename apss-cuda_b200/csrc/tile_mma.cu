@@ -269,7 +269,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_tiles_mma(const TileArgs A, con
         for (int h = 0; h < 2; ++h) {
           // ---- tail of this half-tile
           {
-            const int64_t k0 = A.hptrJ[2 * J + h], k1 = A.hptrJ[2 * J + h + 1];
+            const int64_t k0 = A.hptrJ[kJSegs * J + h * (kJSegs / 2)];
+            const int64_t k1 = A.hptrJ[kJSegs * J + (h + 1) * (kJSegs / 2)];
             if (nch == 1) {
               tail_postings<kBatch>(A, S.ts, T, k0, k1, S.acc, kAccLd, h * kAccCols, ctid, kCT);
             } else {

@@ -35,7 +35,7 @@ struct TileArgs {
   int nbJ;
   const int32_t* blkmaxJ;
   const float* hnormJ;
-  const int64_t* hptrJ;     // postings of each 64-row half-block of J
+  const int64_t* hptrJ;     // postings of each kJSegRows-row segment of J
   const uint2* bilJ_rec;    // packed postings {feature << 8 | row, value bits}
   int p;
   int self;

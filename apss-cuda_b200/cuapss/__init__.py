@@ -543,3 +543,39 @@ def shard_blocks(n: int, shard: int, nshards: int) -> np.ndarray:
     out = np.empty(max(m, 1), np.int32)
     lib().cuapss_shard_blocks(int(n), int(shard), int(nshards), out.ctypes.data, m)
     return out[:m]
+
+
+def read_text(path: str, max_rows: int = -1) -> Csr:
+    """Vectors of a file in the reference's text format (one vector per line,
+    "d v" pairs; main.cu:301-323) as a CSR matrix, rows sorted by feature id,
+    d = largest id + 1 (cuapss_compat_read_text)."""
+    L = lib()
+    f = L.cuapss_compat_text_size
+    f.argtypes = [ctypes.c_char_p, ctypes.c_int64] + [ctypes.POINTER(ctypes.c_int64)] * 3
+    f.restype = ctypes.c_int
+    n, nnz, d = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
+    if f(os.fsencode(path), int(max_rows), ctypes.byref(n), ctypes.byref(nnz),
+         ctypes.byref(d)) != 0:
+        raise ValueError(f"{path}: not in the reference's text format")
+    g = L.cuapss_compat_read_text
+    g.argtypes = [ctypes.c_char_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p,
+                  ctypes.c_void_p]
+    g.restype = ctypes.c_int
+    rp = np.zeros(n.value + 1, np.int64)
+    col = np.empty(max(nnz.value, 1), np.int32)
+    val = np.empty(max(nnz.value, 1), np.float32)
+    if g(os.fsencode(path), int(max_rows), rp.ctypes.data, col.ctypes.data,
+         val.ctypes.data) != 0:
+        raise ValueError(f"{path}: not in the reference's text format")
+    return Csr(rp, col[:nnz.value], val[:nnz.value], max(d.value, 1))
+
+
+def write_text(path: str, x) -> None:
+    """Writes x in the reference's text format (cuapss_compat_write_text)."""
+    f = lib().cuapss_compat_write_text
+    f.argtypes = [ctypes.c_char_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p,
+                  ctypes.c_void_p]
+    f.restype = ctypes.c_int
+    if f(os.fsencode(path), x.n, x.rowptr.ctypes.data, x.col.ctypes.data,
+         x.val.ctypes.data) != 0:
+        raise OSError(f"cannot write {path}")

@@ -64,6 +64,31 @@ int64_t cuapss_compat_tile_ell_to_csr(const int* dim, const float* feature, cons
                                       int sum_vec, int sum_tile, int64_t* rowptr, int32_t* col,
                                       float* val);
 
+/* The reference's input text format (main.cu:301-323): one vector per line.
+ * A line is empty (an empty vector) or one separator character followed by
+ * "d v" pairs (feature id, value; any whitespace between them), each pair
+ * followed by one character: a separator, or the line's newline. The
+ * reference reads it with `input.get(ch); while (ch != '\n') { input >> d >> v;
+ * ...; input.get(ch); }` for each vector.
+ *
+ * cuapss_compat_text_size scans the file: *n_rows = vectors (at most
+ * max_rows when max_rows >= 0), *nnz = their entries, *d = largest feature id
+ * + 1. cuapss_compat_read_text then fills a CSR of those vectors (rowptr
+ * n_rows + 1, col/val nnz), each row sorted by feature id. Both return 0, or
+ * -1 when the file cannot be read or a line is malformed (a token that is
+ * not a number, a negative id, an id repeated within a vector, a missing
+ * value). No counterpart in the reference, which parses inline in main(). */
+int cuapss_compat_text_size(const char* path, int64_t max_rows, int64_t* n_rows, int64_t* nnz,
+                            int64_t* d);
+int cuapss_compat_read_text(const char* path, int64_t max_rows, int64_t* rowptr, int32_t* col,
+                            float* val);
+
+/* Writes n CSR rows in that text format (separator ' ', values printed with
+ * 9 significant digits, which round-trip FP32 exactly). Returns 0, or -1 on
+ * an I/O error. */
+int cuapss_compat_write_text(const char* path, int64_t n, const int64_t* rowptr,
+                             const int32_t* col, const float* val);
+
 #ifdef __cplusplus
 }
 #endif

@@ -35,6 +35,14 @@ def test_every_declared_symbol_is_exported():
     assert set(cuapss.EXPORTED) <= exp
 
 
+def test_every_compat_symbol_is_exported():
+    names = _declared("cuapss_compat.h")
+    assert "cuapss_compat_read_text" in names
+    exp = _exported(cuapss.LIB_PATH)
+    missing = [n for n in names if n not in exp]
+    assert not missing, missing
+
+
 def test_synth_symbols_exported():
     exp = _exported(os.path.join(ROOT, "apss-cuda_b200", "lib", "libcuapss_synth.so"))
     for n in _declared("cuapss_synth.h"):

@@ -136,3 +136,76 @@ def test_similarity_join_device_counts(capfd):
     for a, b, c in lines:
         x_, y_ = ord(a) - 65, (ord(b) - 65 if b else ord(a) - 65)
         assert int(c) == want[8 * x_ + y_]
+
+
+# ---- the reference's text input format (main.cu:301-323) ----
+
+def _reference_lines(x, rng):
+    """Lines as the reference's loader reads them: one leading separator
+    character, then "d v" pairs each followed by one character (a separator
+    or the newline); entries in any order, mixed whitespace inside a pair."""
+    out = []
+    for r in range(x.n):
+        a, b = int(x.rowptr[r]), int(x.rowptr[r + 1])
+        if a == b:
+            out.append("\n")
+            continue
+        parts = []
+        for e in rng.permutation(np.arange(a, b)):
+            gap = " " if rng.uniform() < 0.7 else "\t "
+            parts.append(f"{int(x.col[e])}{gap}{float(x.val[e]):.9g}")
+        sep = "\t" if r % 3 == 0 else " "
+        out.append(sep + sep.join(parts) + "\n")
+    return "".join(out)
+
+
+def test_text_format_reads_reference_lines(tmp_path):
+    x = synth.generate("plain_20k", n=300)
+    # a few empty vectors, as an empty line
+    rp = x.rowptr.copy()
+    keep = np.ones(x.n, bool)
+    keep[[5, 77, 299]] = False
+    lens = np.where(keep, np.diff(rp), 0)
+    idx = np.concatenate([np.arange(rp[r], rp[r + 1]) for r in range(x.n) if keep[r]])
+    y = synth.Csr(np.concatenate([[0], np.cumsum(lens)]), x.col[idx], x.val[idx], x.d)
+    p = tmp_path / "vectors.txt"
+    p.write_text(_reference_lines(y, np.random.default_rng(1)))
+    z = cuapss.read_text(str(p))
+    assert z.n == y.n and z.d == int(y.col.max()) + 1
+    np.testing.assert_array_equal(z.rowptr, y.rowptr)
+    np.testing.assert_array_equal(z.col, y.col)
+    np.testing.assert_array_equal(z.val, y.val)
+    # the first rows only
+    w = cuapss.read_text(str(p), max_rows=10)
+    assert w.n == 10 and w.nnz == int(y.rowptr[10])
+
+
+def test_text_format_round_trip_through_tile_ell(tmp_path):
+    x = synth.generate("plain_20k", n=517)
+    p = tmp_path / "x.txt"
+    cuapss.write_text(str(p), x)
+    y = cuapss.read_text(str(p))
+    np.testing.assert_array_equal(y.rowptr, x.rowptr)
+    np.testing.assert_array_equal(y.col, x.col)
+    np.testing.assert_array_equal(y.val, x.val)
+    # the reference builds its tile-ELL partitions from these vectors
+    dim, feat, ts = to_tile_ell(y, np.random.default_rng(2))
+    m, rp, col, val = convert(dim, feat, ts, y.n)
+    assert m == x.nnz
+    np.testing.assert_array_equal(rp, x.rowptr)
+    np.testing.assert_array_equal(col, x.col)
+    np.testing.assert_array_equal(val, x.val)
+
+
+@pytest.mark.parametrize("bad", [" 3 0.5 3 0.25\n",       # id repeated in a vector
+                                 " 3 0.5 -2 0.25\n",      # negative id
+                                 " 3 0.5 x 0.25\n",       # not a number
+                                 " 3 0.5 7\n"])           # missing value
+def test_text_format_rejects_malformed(tmp_path, bad):
+    p = tmp_path / "bad.txt"
+    p.write_text(" 1 0.5 2 0.5\n" + bad)
+    with pytest.raises(ValueError):
+        cuapss.read_text(str(p))
+    assert cuapss.read_text(str(p), max_rows=1).n == 1
+    with pytest.raises(ValueError):
+        cuapss.read_text(str(tmp_path / "missing.txt"))
