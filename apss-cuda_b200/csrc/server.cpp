@@ -3,14 +3,26 @@
 // admission by the working memory of the batches in flight.
 //
 // Lanes. Each lane is a host thread with its own context (own CUDA stream,
-// own grow-only working memory). A free lane takes, under the queue lock, the
-// longest prefix of queued query requests (in arrival order, stopping at the
-// first queued append) that fits max_batch_rows and the memory budget,
-// concatenates their rows into one batch CSR with one threshold per row, runs
-// it with index_query_rows and hands each request its slice of the sorted
-// output (rows of one request are contiguous in the batch). Lanes run
-// concurrently, so their batches overlap on the GPU; requests that arrive
-// while batches run are picked up by the next lane that frees up.
+// own grow-only working memory). A free lane takes, under the queue lock, a
+// batch of queued query items, concatenates their rows into one batch CSR
+// with one threshold per row, runs it with index_query_rows and hands each
+// item its slice of the sorted output (rows of one item are contiguous in
+// the batch). Lanes run concurrently, so their batches overlap on the GPU;
+// requests that arrive while batches run are picked up by the next lane that
+// frees up.
+//
+// Slices. A query request of more than max_batch_rows rows is queued as
+// slices of at most max_batch_rows consecutive rows, so one large request
+// never holds a lane for longer than one batch, its slices run on several
+// lanes at once, and small requests get on the GPU between them. The
+// request is finished when its last slice is; its pairs are the slices'
+// pairs in slice order (sorted by query row, then index row).
+//
+// Order. Among the query items queued ahead of the first queued append, a
+// lane fills its batch in the order of submit time + kRowMs per row (the
+// item's service cost expressed as age): small requests overtake large ones
+// until those have waited kRowMs per row longer, which bounds how long a
+// large item can be passed over.
 //
 // Admission. The working memory of a batch is estimated from its rows,
 // non-zeros and the head width, plus its expected candidates (a running
@@ -18,8 +30,12 @@
 // output). A batch is admitted while the estimates of all batches in flight
 // stay within hbm_budget; a lone batch is always admitted.
 //
-// Appends are taken in submission order by one lane at a time; queries queued
-// behind an append wait until some lane has taken it.
+// Appends are taken in submission order by one lane at a time, when they
+// are the oldest queued item; queries queued behind an append wait until
+// some lane has taken it. A request is matched against the index rows that
+// existed when the first of its batches started (for a sliced request, the
+// fewest rows any of its slices saw; pairs with rows appended later are
+// dropped), reported in cuapss_request_info.index_rows.
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
@@ -38,6 +54,16 @@ namespace {
 
 using Clock = std::chrono::steady_clock;
 
+struct Request;
+using ReqPtr = std::shared_ptr<Request>;
+
+// The results of one slice of a sliced query request.
+struct Part {
+  std::vector<int32_t> oi, oj;
+  std::vector<float> os;
+  int64_t index_rows = 0;
+};
+
 struct Request {
   uint64_t id = 0;
   bool append = false;
@@ -48,13 +74,19 @@ struct Request {
   std::vector<float> t;
   Clock::time_point submit, start, done;
   bool finished = false;
+  bool started = false;
   cuapss_status status = CUAPSS_OK;
   std::vector<int32_t> oi, oj;
   std::vector<float> os;
   int64_t batch_id = -1, batch_rows = 0, index_rows = 0;
+  // a slice: the request it belongs to, its number and its first row there
+  ReqPtr parent;
+  int slice = 0;
+  int64_t row_off = 0;
+  // a sliced request: its slices' results and how many are still running
+  std::vector<Part> parts;
+  int slices_left = 0;
 };
-
-using ReqPtr = std::shared_ptr<Request>;
 
 double ms_between(Clock::time_point a, Clock::time_point b) {
   return std::chrono::duration<double, std::milli>(b - a).count();
@@ -82,10 +114,74 @@ struct cuapss_server {
 
 namespace {
 
+// Age, in ms, that one query row of an item is worth when batches are
+// filled (see "Order" above).
+constexpr double kRowMs = 0.02;
+
 int64_t estimate_bytes(const cuapss_server* s, int64_t rows, int64_t nnz) {
   const double cand = s->cand_per_row * (double)rows;
   return (int64_t)((double)rows * (2.0 * s->head_width + 256.0) + (double)nnz * 64.0 +
                    cand * 24.0) + (1 << 20);
+}
+
+// Records the outcome of a finished query item (under the server lock): a
+// whole request is finished; a slice fills its part of the request, which
+// is finished with its last slice.
+void finish_item(Request& r, cuapss_status st, std::vector<int32_t>&& oi, std::vector<int32_t>&& oj,
+                 std::vector<float>&& os, int64_t batch_id, int64_t rows, int64_t rows_seen,
+                 Clock::time_point now) {
+  r.rp.clear();
+  r.col.clear();
+  r.val.clear();
+  if (!r.parent) {
+    r.status = st;
+    r.oi = std::move(oi);
+    r.oj = std::move(oj);
+    r.os = std::move(os);
+    r.batch_id = batch_id;
+    r.batch_rows = rows;
+    r.index_rows = rows_seen;
+    r.done = now;
+    r.finished = true;
+    return;
+  }
+  Request& p = *r.parent;
+  Part& part = p.parts[(size_t)r.slice];
+  if (st == CUAPSS_OK) {
+    for (auto& v : oi) v += (int32_t)r.row_off;
+    part.oi = std::move(oi);
+    part.oj = std::move(oj);
+    part.os = std::move(os);
+  } else if (p.status == CUAPSS_OK) {
+    p.status = st;
+  }
+  part.index_rows = rows_seen;
+  p.batch_id = std::max(p.batch_id, batch_id);
+  p.batch_rows = std::max(p.batch_rows, rows);
+  if (--p.slices_left > 0) return;
+  // the last slice: one index view for the request, pairs in slice order
+  int64_t view = INT64_MAX;
+  for (const Part& q : p.parts) view = std::min(view, q.index_rows);
+  p.index_rows = view;
+  if (p.status == CUAPSS_OK) {
+    size_t m = 0;
+    for (const Part& q : p.parts) m += q.oi.size();
+    p.oi.reserve(m);
+    p.oj.reserve(m);
+    p.os.reserve(m);
+    for (Part& q : p.parts) {
+      for (size_t k = 0; k < q.oi.size(); ++k) {
+        if (q.oj[k] >= view) continue;  // a row appended after the request's view
+        p.oi.push_back(q.oi[k]);
+        p.oj.push_back(q.oj[k]);
+        p.os.push_back(q.os[k]);
+      }
+      q = Part();
+    }
+  }
+  p.parts.clear();
+  p.done = now;
+  p.finished = true;
 }
 
 void run_append(cuapss_server* s, cuapss_ctx* ctx, const ReqPtr& r) {
@@ -155,33 +251,28 @@ void run_batch(cuapss_server* s, cuapss_ctx* ctx, std::vector<ReqPtr>& batch, in
     }
     break;
   }
-  // split by request: pairs are sorted by batch row
+  // split by item: pairs are sorted by batch row
   std::vector<size_t> cut(batch.size() + 1, oi.size());
   if (st == CUAPSS_OK) {
     for (size_t k = 0; k <= batch.size(); ++k)
       cut[k] = (size_t)(std::lower_bound(oi.begin(), oi.end(), (int32_t)first[k]) - oi.begin());
   }
+  std::vector<std::vector<int32_t>> pi(batch.size()), pj(batch.size());
+  std::vector<std::vector<float>> ps(batch.size());
+  if (st == CUAPSS_OK) {
+    for (size_t k = 0; k < batch.size(); ++k) {
+      const size_t a = cut[k], b = cut[k + 1];
+      pi[k].resize(b - a);
+      for (size_t m = a; m < b; ++m) pi[k][m - a] = oi[m] - (int32_t)first[k];
+      pj[k].assign(oj.begin() + a, oj.begin() + b);
+      ps[k].assign(os.begin() + a, os.begin() + b);
+    }
+  }
   const Clock::time_point now = Clock::now();
   std::lock_guard<std::mutex> lk(s->mu);
-  for (size_t k = 0; k < batch.size(); ++k) {
-    Request& r = *batch[k];
-    r.status = st;
-    if (st == CUAPSS_OK) {
-      const size_t a = cut[k], b = cut[k + 1];
-      r.oi.resize(b - a);
-      r.oj.assign(oj.begin() + a, oj.begin() + b);
-      r.os.assign(os.begin() + a, os.begin() + b);
-      for (size_t m = a; m < b; ++m) r.oi[m - a] = oi[m] - (int32_t)first[k];
-    }
-    r.batch_id = batch_id;
-    r.batch_rows = rows;
-    r.index_rows = rows_seen;
-    r.done = now;
-    r.finished = true;
-    r.rp.clear();
-    r.col.clear();
-    r.val.clear();
-  }
+  for (size_t k = 0; k < batch.size(); ++k)
+    finish_item(*batch[k], st, std::move(pi[k]), std::move(pj[k]), std::move(ps[k]), batch_id,
+                rows, rows_seen, now);
   if (st == CUAPSS_OK && rows > 0) {
     const double per = (double)stats.candidates / (double)rows;
     s->cand_per_row = 0.8 * s->cand_per_row + 0.2 * per;
@@ -205,28 +296,48 @@ void lane_loop(cuapss_server* s, int lane) {
             app->start = Clock::now();
             break;
           }
-          // longest admissible prefix of query requests
-          int64_t rows = 0, nnz = 0;
-          size_t k = 0;
-          for (; k < s->queue.size(); ++k) {
+          // query items ahead of the first append, cheapest (age + rows) first
+          std::vector<size_t> cand;
+          for (size_t k = 0; k < s->queue.size() && cand.size() < 1024; ++k) {
+            if (s->queue[k]->append) break;
+            cand.push_back(k);
+          }
+          auto key = [&](size_t k) {
             const Request& r = *s->queue[k];
-            if (r.append) break;
+            return std::chrono::duration<double, std::milli>(r.submit.time_since_epoch()).count() +
+                   kRowMs * (double)r.n;
+          };
+          std::stable_sort(cand.begin(), cand.end(),
+                           [&](size_t a, size_t b) { return key(a) < key(b); });
+          int64_t rows = 0, nnz = 0;
+          std::vector<size_t> take;
+          for (size_t k : cand) {
+            const Request& r = *s->queue[k];
             const int64_t nr = rows + r.n, nz = nnz + (int64_t)r.col.size();
-            if (k > 0 && nr > s->opts.max_batch_rows) break;
+            if (!take.empty() && nr > s->opts.max_batch_rows) continue;
             const int64_t e = estimate_bytes(s, nr, nz);
-            if (s->inflight_bytes + e > s->opts.hbm_budget && (k > 0 || s->inflight_bytes > 0))
-              break;
+            if (s->inflight_bytes + e > s->opts.hbm_budget && (!take.empty() || s->inflight_bytes > 0))
+              continue;
             rows = nr;
             nnz = nz;
             est = e;
+            take.push_back(k);
           }
-          if (k > 0) {
+          if (!take.empty()) {
             const Clock::time_point now = Clock::now();
-            for (size_t m = 0; m < k; ++m) {
-              batch.push_back(s->queue.front());
-              s->queue.pop_front();
-              batch.back()->start = now;
+            std::sort(take.begin(), take.end());
+            for (size_t k : take) {
+              ReqPtr r = s->queue[k];
+              r->start = now;
+              Request& owner = r->parent ? *r->parent : *r;
+              if (!owner.started) {
+                owner.started = true;
+                owner.start = now;
+              }
+              batch.push_back(r);
             }
+            for (size_t m = take.size(); m-- > 0;)
+              s->queue.erase(s->queue.begin() + (std::ptrdiff_t)take[m]);
             s->inflight_bytes += est;
             bid = s->next_batch++;
             break;
@@ -261,7 +372,36 @@ uint64_t enqueue(cuapss_server* s, ReqPtr r) {
   r->id = s->next_id++;
   r->submit = Clock::now();
   s->reqs[r->id] = r;
-  s->queue.push_back(r);
+  const int64_t cap = s->opts.max_batch_rows;
+  if (r->append || r->n <= cap) {
+    s->queue.push_back(r);
+  } else {
+    // slices of at most max_batch_rows rows
+    const int ns = (int)((r->n + cap - 1) / cap);
+    r->parts.resize((size_t)ns);
+    r->slices_left = ns;
+    for (int k = 0; k < ns; ++k) {
+      auto sl = std::make_shared<Request>();
+      const int64_t lo = (int64_t)k * cap, hi = std::min(r->n, lo + cap);
+      sl->parent = r;
+      sl->slice = k;
+      sl->row_off = lo;
+      sl->n = hi - lo;
+      sl->d = r->d;
+      sl->submit = r->submit;
+      const int64_t e0 = r->rp[(size_t)lo], e1 = r->rp[(size_t)hi];
+      sl->rp.resize((size_t)(hi - lo) + 1);
+      for (int64_t i = lo; i <= hi; ++i) sl->rp[(size_t)(i - lo)] = r->rp[(size_t)i] - e0;
+      sl->col.assign(r->col.begin() + e0, r->col.begin() + e1);
+      sl->val.assign(r->val.begin() + e0, r->val.begin() + e1);
+      sl->t.assign(r->t.begin() + lo, r->t.begin() + hi);
+      s->queue.push_back(sl);
+    }
+    r->rp.clear();
+    r->col.clear();
+    r->val.clear();
+    r->t.clear();
+  }
   s->cv_work.notify_all();
   return r->id;
 }

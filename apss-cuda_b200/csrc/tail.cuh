@@ -128,8 +128,18 @@ __device__ __forceinline__ TailI stage_tail_chunk(const TileArgs& A, const TailS
   return T;
 }
 
+// Accumulator cell of (row r, column c): plain rows of ld ints, or (SWZ)
+// rows of 32 ints whose 4-int groups are permuted by the row (group g of row
+// r at position g ^ (r % 8)), so that eight consecutive rows' same group sit
+// in distinct banks for the epilogue's 16-byte reads.
+template <bool SWZ>
+__device__ __forceinline__ int acc_cell(int r, int c, int ld) {
+  return SWZ ? r * 32 + ((((c >> 2) ^ (r & 7)) << 2) | (c & 3)) : r * ld + c;
+}
+
 // Products of one J posting (feature f, column c, value v) with the staged
 // I postings of feature f.
+template <bool SWZ>
 __device__ __forceinline__ void tail_probe(const TailStage& S, uint32_t f, int c, float v,
                                            int* acc, int ld) {
   const uint32_t b = f & (kTailBuckets - 1u);
@@ -144,24 +154,24 @@ __device__ __forceinline__ void tail_probe(const TailStage& S, uint32_t f, int c
       continue;
     }
     if (tg == tag) {
-      int* col = acc + c;
       const int ee = e + len;
       for (; e + 1 < ee; e += 2) {
         const uint32_t t0 = S.et[e], t1 = S.et[e + 1];
         const float u0 = S.eu[e], u1 = S.eu[e + 1];
-        atomicAdd(col + (int)(t0 & 127u) * ld, tail_fixed(u0 * v));
-        atomicAdd(col + (int)(t1 & 127u) * ld, tail_fixed(u1 * v));
+        atomicAdd(acc + acc_cell<SWZ>((int)(t0 & 127u), c, ld), tail_fixed(u0 * v));
+        atomicAdd(acc + acc_cell<SWZ>((int)(t1 & 127u), c, ld), tail_fixed(u1 * v));
       }
-      if (e < ee) atomicAdd(col + (int)(S.et[e] & 127u) * ld, tail_fixed(S.eu[e] * v));
+      if (e < ee) atomicAdd(acc + acc_cell<SWZ>((int)(S.et[e] & 127u), c, ld), tail_fixed(S.eu[e] * v));
     }
     break;
   }
 }
 
 // Tail contributions of the J postings [k0, k1) (column = record & 0xff,
-// minus cofs) against the staged chunk, into acc[r * ld + c - cofs]; thread
-// tid of nthreads; NB postings per thread are loaded before they are used.
-template <int NB>
+// minus cofs) against the staged chunk, into acc at acc_cell<SWZ>(r, c - cofs);
+// thread tid of nthreads; NB postings per thread are loaded before they are
+// used.
+template <int NB, bool SWZ = false>
 __device__ __forceinline__ void tail_postings(const TileArgs& A, const TailStage& S,
                                               const TailI& T, int64_t k0, int64_t k1, int* acc,
                                               int ld, int cofs, int tid, int nthreads) {
@@ -177,8 +187,8 @@ __device__ __forceinline__ void tail_postings(const TileArgs& A, const TailStage
 #pragma unroll
     for (int q = 0; q < NB; ++q) {
       if (rec[q].x == 0xffffffffu) break;  // the rest of the batch is past the range
-      tail_probe(S, rec[q].x >> 8, (int)(rec[q].x & 0xffu) - cofs, __uint_as_float(rec[q].y),
-                 acc, ld);
+      tail_probe<SWZ>(S, rec[q].x >> 8, (int)(rec[q].x & 0xffu) - cofs,
+                      __uint_as_float(rec[q].y), acc, ld);
     }
   }
 }

@@ -12,22 +12,34 @@
 // fengyilin118/APSS-CUDA similarity_search.cu:441-506, 854-915).
 //
 // Warp roles (one CTA per SM, persistent over a static share of the units):
-//   warp 0       producer: bulk copies of I and J operand tiles into a
-//                3- or 4-stage shared-memory ring (mbarrier full/empty);
-//   warp 1       MMA: allocates 256 tensor-memory columns (two 128-column
-//                accumulators), one thread issues tcgen05.mma and commits;
-//   warps 2..31  tail: the sparse tail of the tile in fixed point
-//                (tail.cuh), in two 64-column halves; the first 16 of them
-//                then run the epilogue: the accumulator is read with
-//                tcgen05.ld, head + tail is compared with t - eps(i, j) and
-//                candidates are compacted with a warp ballot.
+//   warp 0          producer: bulk copies of I and J operand tiles into a
+//                   3- or 4-stage shared-memory ring (mbarrier full/empty);
+//   warp 1          MMA: allocates 256 tensor-memory columns (two 128-column
+//                   accumulators), one thread issues tcgen05.mma and commits;
+//   kTW tail warps  the sparse tail of each tile in fixed point (tail.cuh),
+//                   one slab of kSlabCols tile columns (one J segment) at a
+//                   time, into one of two shared slab accumulators;
+//   kEW epilogue    two per tensor-memory lane quarter: per slab, the
+//   warps           accumulator columns are read with tcgen05.ld, head +
+//                   tail is compared with t - eps(i, j), candidates are
+//                   compacted with a warp ballot and the slab accumulator is
+//                   cleared and handed back to the tail warps.
+// The tail of slab s + 1 runs while the epilogue drains slab s (and each tail
+// thread's first J postings of slab s + 1 are loaded during slab s), and the MMAs
+// of the next tile run while both work on this one. The hand-offs are
+// mbarriers: afull (tail -> epilogue) and aempty (epilogue -> tail) per slab
+// buffer, tfull (MMA -> epilogue) and tempty (epilogue -> MMA) per tensor
+// memory accumulator.
 // eps(i, j) bounds BF16 input rounding (2^-8 relative per factor) and the
 // FP32 / fixed-point sums, so no pair with FP64 similarity >= t is dropped;
 // the finalize stage decides the band exactly in FP64.
 //
-// Every mbarrier wait is bounded; a timeout raises kErrTimeout, sets a
-// shared abort flag that the other roles poll, drains in-flight copies and
-// MMAs, frees tensor memory and returns.
+// Every mbarrier wait is bounded by device time; a timeout raises
+// kErrTimeout and a shared abort flag that the other roles' waits poll.
+// A tail or epilogue warp that gave up stops working and signalling but still
+// takes part in its group's named barriers, so no warp is left waiting on
+// one; the producer and MMA threads drain their in-flight copies and MMAs,
+// tensor memory is freed and the kernel returns.
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -40,27 +52,36 @@ namespace cuapss {
 
 namespace {
 
-constexpr int kCW = 30;                       // tail warps; the first kEpiW also run the epilogue
-constexpr int kEpiW = 16;                     // epilogue warps (4 per tensor-memory lane quarter)
-constexpr int kCT = kCW * 32;                 // their threads
-constexpr int kThreads = 64 + kCT;            // + producer warp + MMA warp
+constexpr int kTW = 22;                       // tail warps
+constexpr int kEW = 8;                        // epilogue warps, 2 per tensor-memory lane quarter
+constexpr int kTT = kTW * 32;                 // tail threads
+constexpr int kET = kEW * 32;                 // epilogue threads
+constexpr int kFirstEpi = 2 + kTW;            // first epilogue warp
+constexpr int kThreads = 64 + kTT + kET;      // + producer warp + MMA warp
+static_assert(kThreads == 1024, "one CTA of 32 warps per SM");
+static_assert(kFirstEpi % 4 == 0, "epilogue warp w reads tensor-memory lanes 32 (w % 4) ..");
 constexpr int kKC = 64;                       // BF16 features per chunk (128-byte rows)
 constexpr int kTileBytes = kBlockRows * kKC * 2;  // 16 KB per operand chunk
-constexpr int kAccCols = 64;                  // tail accumulator: half a tile
-constexpr int kAccLd = kAccCols + 4;          // 16-byte rows; 8 rows x 272 B cover all banks
+constexpr int kSlabCols = kJSegRows;          // tile columns per slab (one J segment)
+constexpr int kSlabs = kJSegs;                // slabs per tile
+constexpr int kSlabInts = kBlockRows * kSlabCols;  // one slab accumulator
+constexpr int kEpiCols = kSlabCols / (kEW / 4);    // slab columns per epilogue thread (16)
 constexpr uint32_t kTmemCols = 256;
-constexpr int kComputeBar = 1;
+constexpr int kTailBar = 1;
+constexpr int kEpiBar = 2;
 constexpr int kBatch = 4;                     // J postings per thread per load batch
-constexpr int kEpiCols = kAccCols / (kEpiW / 4);  // tile columns per thread per half (16)
+static_assert(kSlabCols == 32, "slab accumulator rows are 32 ints (8 swizzled groups)");
 
 struct SmemM {
   uint8_t* stage;       // STAGES x (A 16 KB | B 16 KB), 1024-byte aligned
-  int* acc;
-  float* hnj;
+  int* acc;             // [2][128][32] slab accumulators (swizzled groups)
+  float* hnj;           // [2][128] per-column head margins of a tile
   uint64_t* full;
   uint64_t* empty;
   uint64_t* tfull;
   uint64_t* tempty;
+  uint64_t* afull;
+  uint64_t* aempty;
   uint64_t* drain;
   uint32_t* tmem_base;
   int* abort;
@@ -73,10 +94,11 @@ __host__ __device__ constexpr size_t align_up(size_t x, size_t a) { return (x + 
 // staged tail postings.
 template <int STAGES, int CAP>
 struct Cfg {
+  static constexpr int kBars = 2 * STAGES + 2 + 2 + 2 + 2 + 1;
   static constexpr size_t kAcc = (size_t)STAGES * 2 * kTileBytes;
-  static constexpr size_t kHnj = align_up(kAcc + (size_t)kBlockRows * kAccLd * 4, 16);
-  static constexpr size_t kBars = align_up(kHnj + (size_t)kBlockRows * 4, 16);
-  static constexpr size_t kTmem = align_up(kBars + (size_t)(2 * STAGES + 5) * 8, 16);
+  static constexpr size_t kHnj = align_up(kAcc + (size_t)2 * kSlabInts * 4, 16);
+  static constexpr size_t kBar = align_up(kHnj + (size_t)2 * kBlockRows * 4, 16);
+  static constexpr size_t kTmem = align_up(kBar + (size_t)kBars * 8, 16);
   static constexpr size_t kAbort = kTmem + 16;
   static constexpr size_t kTail = align_up(kAbort + 16, 16);
   static constexpr size_t kTotal = align_up(kTail + tail_stage_bytes<CAP>(), 16);
@@ -92,12 +114,14 @@ __device__ __forceinline__ SmemM carve(uint8_t* raw) {
   s.stage = base;
   s.acc = reinterpret_cast<int*>(base + C::kAcc);
   s.hnj = reinterpret_cast<float*>(base + C::kHnj);
-  uint64_t* b = reinterpret_cast<uint64_t*>(base + C::kBars);
+  uint64_t* b = reinterpret_cast<uint64_t*>(base + C::kBar);
   s.full = b;
   s.empty = b + STAGES;
   s.tfull = b + 2 * STAGES;
   s.tempty = b + 2 * STAGES + 2;
-  s.drain = b + 2 * STAGES + 4;
+  s.afull = b + 2 * STAGES + 4;
+  s.aempty = b + 2 * STAGES + 6;
+  s.drain = b + 2 * STAGES + 8;
   s.tmem_base = reinterpret_cast<uint32_t*>(base + C::kTmem);
   s.abort = reinterpret_cast<int*>(base + C::kAbort);
   s.ts = tail_stage_at<CAP>(base + C::kTail);
@@ -124,6 +148,55 @@ __device__ __forceinline__ void raise_abort(const TileArgs& A, volatile int* abo
   }
 }
 
+// wait_or_abort for a whole warp: every lane waits (so every lane acquires
+// what the arrivals released) and the warp takes one answer, so it stays
+// converged for its warp-synchronous work; on a give-up the abort is raised.
+// Returns the warp's new `live`.
+__device__ __forceinline__ bool warp_wait(const TileArgs& A, uint64_t* bar, uint32_t parity,
+                                          volatile int* abort, bool live) {
+  bool got = live ? wait_or_abort(bar, parity, abort) : true;
+  got = __all_sync(0xffffffffu, got);
+  if (live && !got && (threadIdx.x & 31) == 0) raise_abort(A, abort);
+  return live && got;
+}
+
+// First batch of a slab's J postings [k0, k1): thread tid of nthreads takes
+// postings tid, tid + nthreads, ...; unused slots hold the end marker.
+template <int NB>
+__device__ __forceinline__ void load_batch(const TileArgs& A, int64_t k0, int64_t k1, int tid,
+                                           int nthreads, uint2 (&rec)[NB]) {
+  const int n = (int)(k1 - k0);
+#pragma unroll
+  for (int q = 0; q < NB; ++q) {
+    const int k = tid + q * nthreads;
+    rec[q] = k < n ? __ldg(&A.bilJ_rec[k0 + k]) : make_uint2(0xffffffffu, 0u);
+  }
+}
+
+template <int NB>
+__device__ __forceinline__ void probe_batch(const TailStage& S, const uint2 (&rec)[NB], int* acc,
+                                            int cofs) {
+#pragma unroll
+  for (int q = 0; q < NB; ++q) {
+    if (rec[q].x == 0xffffffffu) break;  // the rest of the batch is past the range
+    tail_probe<true>(S, rec[q].x >> 8, (int)(rec[q].x & 0xffu) - cofs, __uint_as_float(rec[q].y),
+                     acc, kSlabCols);
+  }
+}
+
+// The postings of a slab past its first batch (long slabs only).
+template <int NB>
+__device__ __forceinline__ void tail_rest(const TileArgs& A, const TailStage& S, const TailI& T,
+                                          int64_t k0, int64_t k1, int* acc, int cofs, int tid,
+                                          int nthreads) {
+  if (k1 - k0 <= (int64_t)NB * nthreads || !T.any) return;
+  for (int64_t kb = k0 + (int64_t)NB * nthreads; kb < k1; kb += (int64_t)NB * nthreads) {
+    uint2 rec[NB];
+    load_batch<NB>(A, kb, k1, tid, nthreads, rec);
+    probe_batch<NB>(S, rec, acc, cofs);
+  }
+}
+
 struct MmaArgs {
   const uint8_t* headI16;
   const uint8_t* headJ16;
@@ -143,7 +216,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_tiles_mma(const TileArgs A, con
     }
     for (int b = 0; b < 2; ++b) {
       mbar_init(&S.tfull[b], 1);
-      mbar_init(&S.tempty[b], kEpiW);
+      mbar_init(&S.tempty[b], kEW);
+      mbar_init(&S.afull[b], kTW);
+      mbar_init(&S.aempty[b], kEW);
     }
     mbar_init(S.drain, 1);
     *abort = 0;
@@ -154,7 +229,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_tiles_mma(const TileArgs A, con
     tmem_relinquish();
   }
   if (warp >= 2)
-    for (int i = threadIdx.x - 64; i < kBlockRows * kAccLd; i += kCT) S.acc[i] = 0;
+    for (int i = threadIdx.x - 64; i < 2 * kSlabInts; i += kTT + kET) S.acc[i] = 0;
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
@@ -235,88 +310,121 @@ __global__ void __launch_bounds__(kThreads, 1) k_tiles_mma(const TileArgs A, con
       }
     }
     __syncwarp();
+  } else if (warp < kFirstEpi) {
+    // ------------------------------------------------------------- tail
+    // Each thread keeps the first batch of the next slab's J postings in
+    // registers (loaded while it works on this slab), so the load latency
+    // of a slab's records overlaps the previous slab's probes.
+    const int ttid = threadIdx.x - 64;
+    bool live = true;
+    uint32_t g = 0;  // slabs processed by this CTA
+    for (int u = blockIdx.x; u < A.nunits; u += gridDim.x) {
+      const int4 U = A.units[u];
+      if (U.y >= U.z) continue;
+      const int I = U.x;
+      named_bar(kTailBar, kTT);  // every tail warp is done with the previous unit's staging
+      const int nch = tail_nchunks<CAP>(A, I);
+      TailI T{};
+      if (nch == 1) T = stage_tail_chunk<kTT, kTailBar, CAP>(A, S.ts, I, 0, ttid);
+      uint2 nxt[kBatch];
+      load_batch<kBatch>(A, A.hptrJ[kJSegs * U.y], A.hptrJ[kJSegs * U.y + 1], ttid, kTT, nxt);
+      for (int J = U.y; J < U.z; ++J) {
+        for (int q = 0; q < kSlabs; ++q, ++g) {
+          const uint32_t k = g & 1u, use = g >> 1;
+          const int64_t k0 = A.hptrJ[kJSegs * J + q], k1 = A.hptrJ[kJSegs * J + q + 1];
+          uint2 cur[kBatch];
+#pragma unroll
+          for (int b = 0; b < kBatch; ++b) cur[b] = nxt[b];
+          // the next slab of this unit: its first batch, in flight from here
+          const int qn = q + 1 < kSlabs ? q + 1 : 0, Jn = q + 1 < kSlabs ? J : J + 1;
+          if (Jn < U.z)
+            load_batch<kBatch>(A, A.hptrJ[kJSegs * Jn + qn], A.hptrJ[kJSegs * Jn + qn + 1], ttid,
+                               kTT, nxt);
+          live = warp_wait(A, &S.aempty[k], (use & 1u) ^ 1u, abort, live);
+          int* acc = S.acc + k * kSlabInts;
+          const int cofs = q * kSlabCols;
+          if (nch == 1) {
+            if (live && T.any) {
+              probe_batch<kBatch>(S.ts, cur, acc, cofs);
+              tail_rest<kBatch>(A, S.ts, T, k0, k1, acc, cofs, ttid, kTT);
+            }
+          } else {
+            for (int c = 0; c < nch; ++c) {
+              const TailI Tc = stage_tail_chunk<kTT, kTailBar, CAP>(A, S.ts, I, c, ttid);
+              if (live && Tc.any) {
+                probe_batch<kBatch>(S.ts, cur, acc, cofs);
+                tail_rest<kBatch>(A, S.ts, Tc, k0, k1, acc, cofs, ttid, kTT);
+              }
+              named_bar(kTailBar, kTT);  // staging rewritten by the next chunk
+            }
+          }
+          __syncwarp();
+          if (live && lane == 0) mbar_arrive(&S.afull[k]);
+        }
+      }
+    }
   } else {
-    // ---------------------------------------------- tail + epilogue warps
-    const int ctid = threadIdx.x - 64;
-    const bool epi = (warp - 2) < kEpiW;  // this warp also runs the epilogue
-    const int q = warp & 3;             // tensor-memory lane quarter of this warp
-    const int colq = (warp - 2) >> 2;   // which kEpiCols of each 64 columns
-    const int row = 32 * q + lane;
-    uint32_t tt = 0;
-    bool ok = true;
-    for (int u = blockIdx.x; ok && u < A.nunits; u += gridDim.x) {
+    // --------------------------------------------------------- epilogue
+    const int ew = warp - kFirstEpi;
+    const int etid = threadIdx.x - (64 + kTT);
+    const int q4 = warp & 3;         // tensor-memory lane quarter of this warp
+    const int colh = ew >> 2;        // which kEpiCols columns of each slab
+    const int row = 32 * q4 + lane;  // tile row of this thread
+    bool live = true;
+    uint32_t tt = 0, g = 0;
+    for (int u = blockIdx.x; u < A.nunits; u += gridDim.x) {
       const int4 U = A.units[u];
       if (U.y >= U.z) continue;
       const int I = U.x;
       const int64_t row0 = (int64_t)I * kBlockRows;
       const int rowsI = (int)(A.nI - row0 < kBlockRows ? A.nI - row0 : kBlockRows);
-      named_bar(kComputeBar, kCT);
-      const int nch = tail_nchunks<CAP>(A, I);
-      TailI T{};
-      if (nch == 1) T = stage_tail_chunk<kCT, kComputeBar, CAP>(A, S.ts, I, 0, ctid);
-      const float hn_r = row < rowsI ? A.hnormI[row0 + row] : 0.0f;
-      const double t_r = A.t_row ? (row < rowsI ? (double)A.t_row[row0 + row] : 2.0) : (double)A.t;
-      for (int J = U.y; ok && J < U.z; ++J, ++tt) {
+      const bool row_ok = row < rowsI;
+      const float hn_r = row_ok ? A.hnormI[row0 + row] : 0.0f;
+      const double t_r = A.t_row ? (row_ok ? (double)A.t_row[row0 + row] : 2.0) : (double)A.t;
+      for (int J = U.y; J < U.z; ++J, ++tt) {
         const uint32_t b = tt & 1u, tround = tt >> 1;
         const int64_t col0 = (int64_t)J * kBlockRows;
         const int colsJ = (int)(A.nJ - col0 < kBlockRows ? A.nJ - col0 : kBlockRows);
         const bool diag = A.self && (I == J);
+        const bool simple = !diag && colsJ == kBlockRows;
         const int kmax = min(A.blkmaxI[I], A.blkmaxJ[J]);
         const float t_lo = __double2float_rd(t_r - (A.eps_c1 * kmax + A.eps_c0));
-        if (ctid < kBlockRows)
-          S.hnj[ctid] =
-              ctid < colsJ ? __double2float_ru(A.eps_head * (double)A.hnormJ[col0 + ctid]) : 0.0f;
-        for (int h = 0; h < 2; ++h) {
-          // ---- tail of this half-tile
-          {
-            const int64_t k0 = A.hptrJ[kJSegs * J + h * (kJSegs / 2)];
-            const int64_t k1 = A.hptrJ[kJSegs * J + (h + 1) * (kJSegs / 2)];
-            if (nch == 1) {
-              tail_postings<kBatch>(A, S.ts, T, k0, k1, S.acc, kAccLd, h * kAccCols, ctid, kCT);
-            } else {
-              for (int c = 0; c < nch; ++c) {
-                const TailI Tc = stage_tail_chunk<kCT, kComputeBar, CAP>(A, S.ts, I, c, ctid);
-                tail_postings<kBatch>(A, S.ts, Tc, k0, k1, S.acc, kAccLd, h * kAccCols, ctid,
-                                      kCT);
-                named_bar(kComputeBar, kCT);  // staging rewritten by the next chunk
-              }
-            }
-          }
-          named_bar(kComputeBar, kCT);
-          if (h == 0) {
-            const bool got = wait_or_abort(&S.tfull[b], tround & 1u, abort);
-            if (named_bar_or(kComputeBar, kCT, !got)) {
-              raise_abort(A, abort);
-              ok = false;
-              break;
-            }
-            tc_fence_after();
-          }
-          if (epi) {
-            // ---- epilogue: head (tensor memory) + tail (shared) vs t - eps
-            const int cbase = h * kAccCols + colq * kEpiCols;  // first tile column of this thread
+        float* hnj = S.hnj + (tt & 1u) * kBlockRows;
+        if (etid < kBlockRows)
+          hnj[etid] =
+              etid < colsJ ? __double2float_ru(A.eps_head * (double)A.hnormJ[col0 + etid]) : 0.0f;
+        named_bar(kEpiBar, kET);
+        live = warp_wait(A, &S.tfull[b], tround & 1u, abort, live);
+        tc_fence_after();
+        for (int q = 0; q < kSlabs; ++q, ++g) {
+          const uint32_t k = g & 1u, use = g >> 1;
+          live = warp_wait(A, &S.afull[k], use & 1u, abort, live);
+          if (live) {
+            // ---- head (tensor memory) + tail (slab accumulator) vs t - eps
+            const int cbase = q * kSlabCols + colh * kEpiCols;  // first tile column
             uint32_t v[kEpiCols];
-            tmem_ld16(
-                tmem + b * (uint32_t)kBlockRows + (uint32_t)cbase + ((uint32_t)(32 * q) << 16), v);
+            tmem_ld16(tmem + b * (uint32_t)kBlockRows + (uint32_t)cbase +
+                          ((uint32_t)(32 * q4) << 16),
+                      v);
+            int* arow = S.acc + k * kSlabInts + row * kSlabCols;
+            const float4* hn4 = reinterpret_cast<const float4*>(hnj + cbase);
             uint32_t pass = 0;
-            int4* arow = reinterpret_cast<int4*>(S.acc + row * kAccLd + colq * kEpiCols);
-            const float4* hn4 = reinterpret_cast<const float4*>(S.hnj + cbase);
-            const bool row_ok = row < rowsI;
-            const bool simple = !diag && colsJ == kBlockRows;
-  #pragma unroll
+#pragma unroll
             for (int j4 = 0; j4 < kEpiCols / 4; ++j4) {
-              const int4 t4 = arow[j4];
-              arow[j4] = make_int4(0, 0, 0, 0);
+              const int grp = colh * (kEpiCols / 4) + j4;  // logical 4-column group
+              int4* cell = reinterpret_cast<int4*>(arow + ((grp ^ (row & 7)) << 2));
+              const int4 t4 = *cell;
+              *cell = make_int4(0, 0, 0, 0);
               const float4 h4 = hn4[j4];
               const int tq[4] = {t4.x, t4.y, t4.z, t4.w};
               const float hh[4] = {h4.x, h4.y, h4.z, h4.w};
-  #pragma unroll
-              for (int k = 0; k < 4; ++k) {
-                const int j = 4 * j4 + k;
+#pragma unroll
+              for (int kk = 0; kk < 4; ++kk) {
+                const int j = 4 * j4 + kk;
                 const int c = cbase + j;
-                const float s = fmaf(__int2float_rn(tq[k]), kTailUnscale, __uint_as_float(v[j]));
+                const float s = fmaf(__int2float_rn(tq[kk]), kTailUnscale, __uint_as_float(v[j]));
                 v[j] = __float_as_uint(s);
-                const float thr = __fmaf_rd(-hn_r, hh[k], t_lo);
+                const float thr = __fmaf_rd(-hn_r, hh[kk], t_lo);
                 bool okp = (s >= thr) && row_ok;
                 if (!simple) okp = okp && (c < colsJ) && (!diag || c > row);
                 pass |= (uint32_t)okp << j;
@@ -325,7 +433,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_tiles_mma(const TileArgs A, con
             if (__any_sync(0xffffffffu, pass != 0u)) {
               const int mine = __popc(pass);
               int incl = mine;
-  #pragma unroll
+#pragma unroll
               for (int o = 1; o < 32; o <<= 1) {
                 const int x = __shfl_up_sync(0xffffffffu, incl, o);
                 if (lane >= o) incl += x;
@@ -335,7 +443,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_tiles_mma(const TileArgs A, con
               if (lane == 31) base = atomicAdd(A.cand_count, (unsigned long long)total);
               base = __shfl_sync(0xffffffffu, base, 31);
               unsigned long long w = base + (unsigned long long)(incl - mine);
-  #pragma unroll
+#pragma unroll
               for (int j = 0; j < kEpiCols; ++j) {
                 if ((pass >> j) & 1u) {
                   if ((int64_t)w < A.cand_cap) {
@@ -348,12 +456,12 @@ __global__ void __launch_bounds__(kThreads, 1) k_tiles_mma(const TileArgs A, con
               }
             }
           }
-          named_bar(kComputeBar, kCT);  // accumulator half cleared
+          __syncwarp();
+          if (live && lane == 0) mbar_arrive(&S.aempty[k]);
         }
-        if (!ok) break;
         tc_fence_before();
         __syncwarp();
-        if (lane == 0 && epi) mbar_arrive(&S.tempty[b]);
+        if (live && lane == 0) mbar_arrive(&S.tempty[b]);
       }
     }
   }

@@ -1,6 +1,7 @@
 """Request server (cuapss_server_*): every request's result in the mix of
 concurrent batches and appends equals the same query run alone against the
-rows it was matched against, within the similarity tolerance."""
+rows it was matched against, within the similarity tolerance -- also when
+requests larger than the batch cap run as slices on several lanes."""
 import numpy as np
 import pytest
 
@@ -50,8 +51,9 @@ def workload(seed, n_requests=60, n_appends=4):
     return base, reqs
 
 
-@pytest.mark.parametrize("lanes,max_rows,budget", [(3, 512, 16 << 30), (2, 4096, 1)],
-                         ids=["three_lanes", "tiny_budget"])
+@pytest.mark.parametrize("lanes,max_rows,budget", [(3, 512, 16 << 30), (2, 4096, 1),
+                                                   (3, 48, 16 << 30)],
+                         ids=["three_lanes", "tiny_budget", "sliced"])
 def test_mix_equals_alone(ctx, lanes, max_rows, budget):
     base, reqs = workload(seed=lanes)
     with cuapss.Index(ctx, base) as idx:
@@ -69,8 +71,9 @@ def test_mix_equals_alone(ctx, lanes, max_rows, budget):
             assert info["status"] == cuapss.OK
             if kind == "append":
                 continue
-            assert info["batch_rows"] >= x.n
-            multi += info["batch_rows"] > x.n
+            # a request of more than max_rows rows runs as slices of max_rows
+            assert info["batch_rows"] >= min(x.n, max_rows)
+            multi += info["batch_rows"] > min(x.n, max_rows)
             # alone: the same query against the index now, restricted to the
             # rows this request was matched against
             ai, aj, as_ = idx.query(x, t)
