@@ -39,15 +39,39 @@ void record_cuda_error(cudaError_t e, const char* what, const char* file, int li
 
 const char* last_error_message() { return g_last_error; }
 
-int choose_head_width(int precision, int64_t n, int64_t d, int64_t nnz) {
-  (void)n;
-  (void)nnz;
-  // measured on the lognormal/Zipf workloads: the tensor-core head is cheap,
-  // so a wide head shrinks the sparse tail; the FP32 head pays per feature
-  int p = precision == CUAPSS_PREC_MIXED ? 1024 : 64;
+// Per-tile cost model of the mixed-precision tile kernel, whose tensor-core
+// side and sparse-tail side overlap, so the slower one sets the pace:
+//   head  kHeadChunkNs per 64 head features (operand stream and MMAs of a
+//         128 x 128 tile),
+//   tail  kTailPostingNs per tail posting of the J block (one probe of the
+//         staged I postings); a block holds 128 x (tail non-zeros per row).
+// The head width p minimises max(head, tail) over multiples of 64; the tail
+// non-zeros at each p come from the posting counts in frequency order.
+constexpr double kHeadChunkNs = 440.0;
+constexpr double kTailPostingNs = 1.04;
+constexpr int kMaxModelHead = 8192;
+
+int choose_head_width(int precision, int64_t n, int64_t d, int64_t nnz,
+                      const std::vector<int64_t>& prefix) {
   const int64_t cap = ((d + 31) / 32) * 32;
-  if (p > cap) p = (int)cap;
-  return p;
+  // the FP32 head runs on CUDA cores and pays per feature per pair: its
+  // measured optimum on the lognormal/Zipf workloads is a narrow head
+  if (precision != CUAPSS_PREC_MIXED) return (int)std::min<int64_t>(64, cap);
+  if (n <= 0 || prefix.size() < 2) return (int)std::min<int64_t>(1024, ((d + 63) / 64) * 64);
+  double best = 1e300;
+  int best_p = 64;
+  const int64_t top = (int64_t)prefix.size() - 1;  // ranks with known counts
+  for (int64_t p = 64; p <= std::min<int64_t>(top, kMaxModelHead); p += 64) {
+    const double tail_per_row = (double)(nnz - prefix[(size_t)p]) / (double)n;
+    const double head = kHeadChunkNs * (double)(p / 64);
+    const double tail = kTailPostingNs * kBlockRows * tail_per_row;
+    const double cost = std::max(head, tail);
+    if (cost < best - 1e-9) {
+      best = cost;
+      best_p = (int)p;
+    }
+  }
+  return best_p;
 }
 
 cuapss_status stage_csr(cuapss_ctx* ctx, const cuapss_csr* x, const std::string& tag,
@@ -106,6 +130,7 @@ cuapss_status join_device(cuapss_ctx* ctx, const DevCsr& a, const DevCsr* b, flo
   const int64_t d = a.d;
   const int64_t launches0 = g_launches.load();
   cudaEventRecord(ctx->ev[0], st);
+  StageRange nvtx("cuapss_run:prepare");
   // ---- validate + posting counts + frequency remap ----
   int32_t* counts = nullptr;
   int32_t* perm = nullptr;
@@ -123,8 +148,14 @@ cuapss_status join_device(cuapss_ctx* ctx, const DevCsr& a, const DevCsr* b, flo
     nrm_b = nrm_a;
   ST_TRY(feature_perm(counts, d, a.n + (self ? 0 : bb.n), ctx->opts.remap, perm, ws, st));
   const int precision = ctx->opts.precision;
-  int p = ctx->opts.head_width > 0 ? ctx->opts.head_width
-                                   : choose_head_width(precision, a.n + bb.n, d, a.nnz + bb.nnz);
+  int p = ctx->opts.head_width;
+  if (p <= 0) {
+    std::vector<int64_t> prefix;
+    if (precision == CUAPSS_PREC_MIXED)
+      ST_TRY(rank_count_prefix(counts, d, ctx->opts.remap, kMaxModelHead, ws, st, &prefix));
+    const int64_t n_all = a.n + (self ? 0 : bb.n), nnz_all = a.nnz + (self ? 0 : bb.nnz);
+    p = choose_head_width(precision, n_all, d, nnz_all, prefix);
+  }
   const bool mixed = precision == CUAPSS_PREC_MIXED;
   const int pq = mixed ? 64 : 32;  // head width granularity of the tile kernels
   p = (int)std::min<int64_t>(((int64_t)p + pq - 1) / pq * pq, ((d + pq - 1) / pq) * pq);
@@ -158,6 +189,7 @@ cuapss_status join_device(cuapss_ctx* ctx, const DevCsr& a, const DevCsr* b, flo
     SJ = &SB;
   }
   cudaEventRecord(ctx->ev[1], st);
+  nvtx.next("cuapss_run:tiles");
   // ---- pair tiles ----
   const double nrm2 = nrm_a * nrm_b;
   TileArgs ta{};
@@ -251,6 +283,7 @@ cuapss_status join_device(cuapss_ctx* ctx, const DevCsr& a, const DevCsr* b, flo
     if (attempt == 2) return CUAPSS_ENOMEM;
   }
   cudaEventRecord(ctx->ev[2], st);
+  nvtx.next("cuapss_run:finalize");
   // ---- finalize: exact decision, reported similarity, sorted output ----
   uint64_t* okey = nullptr;
   uint32_t* oidx = nullptr;

@@ -7,9 +7,12 @@
 // side (remapped rows, head block of its own width p, block-local inverted
 // lists). The units of work, (I block, J block range) pairs, only pair blocks
 // of the same instance, and each I block carries its instance's threshold.
-// One persistent tile launch per bucket; the launches of all buckets are
-// captured in one CUDA graph (updated in place when the next batch has the
-// same topology). Finalize runs per bucket into one pair list, sorted once.
+// One persistent tile launch per bucket, each after the first a programmatic
+// dependent launch of the one before: its CTAs start on the SMs the previous
+// bucket's CTAs leave, so the buckets run as one continuous pass over the
+// SMs. The launches of all buckets are captured in one CUDA graph (updated in
+// place when the next batch has the same topology). Finalize runs per bucket
+// into one pair list, sorted once.
 //
 // The autotuner picks p per bucket: the first time a bucket with given
 // precision, mean row nnz and d is seen, each candidate width is timed
@@ -235,10 +238,15 @@ cuapss_status prepare_bucket(cuapss_ctx* ctx, const BatchIn& in, Bucket& b, int 
   return CUAPSS_OK;
 }
 
-cuapss_status launch_bucket(const Bucket& b, bool mixed, cudaStream_t st) {
+// overlap_prev: this bucket's launch follows another bucket's tile launch
+// and may start on the SMs that launch's CTAs leave (the buckets write
+// disjoint candidate regions and counters), so the buckets run as one
+// continuous persistent pass without an idle tail between launches.
+cuapss_status launch_bucket(const Bucket& b, bool mixed, cudaStream_t st, bool overlap_prev) {
   if (b.ntiles == 0) return CUAPSS_OK;
-  if (mixed) return launch_tiles_mma(b.ta, b.S.head16, b.S.head16, b.p, b.grid, st);
-  return launch_tiles_fp32(b.ta, b.grid, st);
+  if (mixed)
+    return launch_tiles_mma(b.ta, b.S.head16, b.S.head16, b.p, b.grid, st, overlap_prev);
+  return launch_tiles_fp32(b.ta, b.grid, st, overlap_prev);
 }
 
 // Counters of one batch launch: per bucket unit counter and candidate count,
@@ -299,7 +307,7 @@ cuapss_status tune_bucket(cuapss_ctx* ctx, const BatchIn& in, const Bucket& full
     CU_TRY(cudaMemsetAsync(cnt.unit, 0, sizeof(int), st));
     CU_TRY(cudaMemsetAsync(cnt.cand, 0, sizeof(unsigned long long), st));
     CU_TRY(cudaMemsetAsync(cnt.err, 0, sizeof(int), st));
-    ST_TRY(launch_bucket(smp, in.mixed, st));
+    ST_TRY(launch_bucket(smp, in.mixed, st, false));
     int herr = 0;
     CU_TRY(cudaMemcpyAsync(&herr, cnt.err, sizeof(int), cudaMemcpyDeviceToHost, st));
     CU_TRY(cudaStreamSynchronize(st));
@@ -333,8 +341,11 @@ cuapss_status launch_graph(cuapss_ctx* ctx, std::vector<Bucket>& bk, bool mixed,
       cudaMemsetAsync(cnt.cand, 0, sizeof(unsigned long long) * kNumBuckets, st) != cudaSuccess ||
       cudaMemsetAsync(cnt.err, 0, sizeof(int), st) != cudaSuccess)
     s = CUAPSS_ECUDA;
-  for (auto& b : bk)
-    if (s == CUAPSS_OK) s = launch_bucket(b, mixed, st);
+  bool after_tiles = false;
+  for (auto& b : bk) {
+    if (s == CUAPSS_OK) s = launch_bucket(b, mixed, st, after_tiles);
+    after_tiles = after_tiles || b.ntiles > 0;
+  }
   const cudaError_t e = cudaStreamEndCapture(st, &g);
   if (s != CUAPSS_OK) {
     if (g) cudaGraphDestroy(g);
@@ -377,6 +388,7 @@ cuapss_status batch_device(cuapss_ctx* ctx, const DevCsr& x, int k, const int64_
   const bool mixed = ctx->opts.precision == CUAPSS_PREC_MIXED;
   const int64_t launches0 = g_launches.load();
   cudaEventRecord(ctx->ev[0], st);
+  StageRange nvtx("cuapss_batch_run:prepare");
   // ---- validate + posting counts + frequency remap over all instances
   int32_t* counts = nullptr;
   int32_t* perm = nullptr;
@@ -453,6 +465,7 @@ cuapss_status batch_device(cuapss_ctx* ctx, const DevCsr& x, int k, const int64_
   if (bucket_p)
     for (int b = 0; b < kNumBuckets; ++b) bucket_p[b] = used_p[b];
   cudaEventRecord(ctx->ev[1], st);
+  nvtx.next("cuapss_batch_run:tiles");
   // ---- tiles: all buckets in one graph launch; candidate regions per bucket
   int64_t ntiles = 0, nslots = 0;
   for (auto& b : bk) {
@@ -507,6 +520,7 @@ cuapss_status batch_device(cuapss_ctx* ctx, const DevCsr& x, int k, const int64_
   int64_t ncand = 0;
   for (size_t i = 0; i < bk.size(); ++i) ncand += (int64_t)hc[i];
   cudaEventRecord(ctx->ev[2], st);
+  nvtx.next("cuapss_batch_run:finalize");
   // ---- finalize per bucket into one list, then one sort
   uint64_t* okey = nullptr;
   uint32_t* oidx = nullptr;

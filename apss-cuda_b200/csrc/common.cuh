@@ -10,6 +10,7 @@
 #include <string>
 
 #include "cuapss.h"
+#include <nvtx3/nvToolsExt.h>
 
 namespace cuapss {
 
@@ -140,6 +141,21 @@ class Workspace {
     size_t size;
   };
   std::map<std::string, Buf> bufs_;
+};
+
+// NVTX ranges of a call's host-side stages (prepare, tiles, finalize), for
+// Nsight timelines; without a tool attached they cost a few instructions.
+// The current stage's range ends when the next begins or at scope exit.
+class StageRange {
+ public:
+  explicit StageRange(const char* name) { nvtxRangePushA(name); }
+  void next(const char* name) {
+    nvtxRangePop();
+    nvtxRangePushA(name);
+  }
+  ~StageRange() { nvtxRangePop(); }
+  StageRange(const StageRange&) = delete;
+  StageRange& operator=(const StageRange&) = delete;
 };
 
 }  // namespace cuapss

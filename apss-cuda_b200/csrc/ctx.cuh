@@ -5,6 +5,7 @@
 
 #include <map>
 #include <string>
+#include <vector>
 
 #include "common.cuh"
 #include "cuapss.h"
@@ -45,7 +46,10 @@ cuapss_status join_device(cuapss_ctx* ctx, const DevCsr& a, const DevCsr* b, flo
                           cuapss_pairs* out, cuapss_stats* stats, int shard = 0,
                           int nshards = 1);
 
-// Head width used when the options leave it to the library.
-int choose_head_width(int precision, int64_t n, int64_t d, int64_t nnz);
+// Head width used when the options leave it to the library: n rows, nnz
+// non-zeros over d features; prefix[k] = postings of the k most frequent
+// features (rank_count_prefix; may be empty for FP32).
+int choose_head_width(int precision, int64_t n, int64_t d, int64_t nnz,
+                      const std::vector<int64_t>& prefix);
 
 }  // namespace cuapss

@@ -173,6 +173,16 @@ __global__ void k_perm_from_sorted(const uint32_t* __restrict__ sorted_f, int64_
     perm[sorted_f[r]] = (int32_t)r;
 }
 
+// out[r] = posting count of the feature of rank r (sorted_f: ids in rank
+// order, or null for the identity order), r < m.
+__global__ void k_rank_counts(const uint32_t* __restrict__ sorted_f,
+                              const int32_t* __restrict__ counts, int64_t m,
+                              int32_t* __restrict__ out) {
+  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < m;
+       r += (int64_t)gridDim.x * blockDim.x)
+    out[r] = counts[sorted_f ? (int64_t)sorted_f[r] : r];
+}
+
 __global__ void k_iota_i32(int32_t* v, int64_t n) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x)
@@ -738,6 +748,24 @@ cuapss_status feature_perm(const int32_t* counts, int64_t d, int64_t max_count, 
   ST_TRY(radix_sort_pairs(keys, vals, d, fbits + bits_for((uint64_t)max_count), ws, "perm", st));
   k_perm_from_sorted<<<grid_for(d, kThreads), kThreads, 0, st>>>(vals, d, perm);
   LAUNCH_CHECK();
+  return CUAPSS_OK;
+}
+
+cuapss_status rank_count_prefix(const int32_t* counts, int64_t d, int remap, int64_t m,
+                                Workspace& ws, cudaStream_t st, std::vector<int64_t>* prefix) {
+  m = std::max<int64_t>(0, std::min(m, d));
+  prefix->assign((size_t)m + 1, 0);
+  if (m == 0) return CUAPSS_OK;
+  uint32_t* vals = nullptr;
+  if (remap) ST_TRY(ws.get("perm:vals", (size_t)d, &vals));  // ids by rank (feature_perm)
+  int32_t* out = nullptr;
+  ST_TRY(ws.get("perm:rank_counts", (size_t)m, &out));
+  k_rank_counts<<<grid_for(m, kThreads), kThreads, 0, st>>>(remap ? vals : nullptr, counts, m, out);
+  LAUNCH_CHECK();
+  std::vector<int32_t> h((size_t)m);
+  CU_TRY(cudaMemcpyAsync(h.data(), out, sizeof(int32_t) * m, cudaMemcpyDeviceToHost, st));
+  CU_TRY(cudaStreamSynchronize(st));
+  for (int64_t r = 0; r < m; ++r) (*prefix)[(size_t)r + 1] = (*prefix)[(size_t)r] + h[(size_t)r];
   return CUAPSS_OK;
 }
 

@@ -3,6 +3,7 @@
 #pragma once
 
 #include <string>
+#include <vector>
 
 #include "common.cuh"
 #include "side.cuh"
@@ -26,6 +27,11 @@ cuapss_status validate_csr(const int64_t* rp, const int32_t* col, const float* v
 // perm[f] = rank of feature f by (count desc, id asc); identity if !remap.
 cuapss_status feature_perm(const int32_t* counts, int64_t d, int64_t max_count, int remap,
                            int32_t* perm, Workspace& ws, cudaStream_t st);
+
+// Host prefix sums of the posting counts in rank order, after feature_perm:
+// (*prefix)[k] = postings of the k most frequent features, k = 0 .. min(m, d).
+cuapss_status rank_count_prefix(const int32_t* counts, int64_t d, int remap, int64_t m,
+                                Workspace& ws, cudaStream_t st, std::vector<int64_t>* prefix);
 
 // Builds every array of `s` (s.rp0/col0/val0/n/d/nnz must be set).
 cuapss_status build_side(Side& s, const PrepOptions& o, const int32_t* perm, Workspace& ws,

@@ -73,6 +73,13 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity,
   return false;
 }
 
+// Lets the launches that follow this grid on its stream with programmatic
+// serialization start as soon as every CTA of this grid has executed this
+// (or exited): their CTAs then take the SMs this grid's CTAs leave.
+__device__ __forceinline__ void allow_dependent_launch() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 // One-dimensional bulk copy global -> shared, completion counted in bytes on
 // `bar`. dst, src 16-byte aligned; bytes a multiple of 16.
 __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes,

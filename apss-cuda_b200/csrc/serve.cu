@@ -287,8 +287,13 @@ extern "C" cuapss_status cuapss_index_create(cuapss_ctx* ctx, const cuapss_csr* 
   if (nrm >= 1.37) return CUAPSS_EINVAL;  // norms^2 < 1.9 for the fixed-point tail
   ST_TRY(idx->heap.alloc((size_t)a.d, &idx->perm));
   ST_TRY(feature_perm(counts, a.d, a.n, ctx->opts.remap, idx->perm, ctx->ws, ctx->stream));
-  int p = ctx->opts.head_width > 0 ? ctx->opts.head_width
-                                   : choose_head_width(ctx->opts.precision, a.n, a.d, a.nnz);
+  int p = ctx->opts.head_width;
+  if (p <= 0) {
+    std::vector<int64_t> prefix;
+    if (idx->mixed)
+      ST_TRY(rank_count_prefix(counts, a.d, ctx->opts.remap, 8192, ctx->ws, ctx->stream, &prefix));
+    p = choose_head_width(ctx->opts.precision, a.n, a.d, a.nnz, prefix);
+  }
   const int pq = idx->mixed ? 64 : 32;
   p = (int)std::min<int64_t>(((int64_t)p + pq - 1) / pq * pq, ceil_div(a.d, pq) * pq);
   if (idx->mixed && p < 64) p = 64;
@@ -400,6 +405,7 @@ cuapss_status cuapss::index_query_rows(cuapss_ctx* ctx, const cuapss_index* idx,
   Workspace& ws = ctx->ws;
   const int64_t launches0 = g_launches.load();
   cudaEventRecord(ctx->ev[0], st);
+  StageRange nvtx("cuapss_index_query:prepare");
   SegList segs;
   int64_t rows = 0;
   double nrm_idx = 1.0;
@@ -437,6 +443,7 @@ cuapss_status cuapss::index_query_rows(cuapss_ctx* ctx, const cuapss_index* idx,
     CU_TRY(cudaMemcpyAsync(t_row, t, sizeof(float) * q.n, cudaMemcpyHostToDevice, st));
   ST_TRY(tiles_init(idx->mixed));
   cudaEventRecord(ctx->ev[1], st);
+  nvtx.next("cuapss_index_query:tiles");
   // ---- tiles: one launch per segment, candidate region per segment
   const size_t ns = segs.size();
   std::vector<TileArgs> tas(ns);
@@ -530,6 +537,10 @@ cuapss_status cuapss::index_query_rows(cuapss_ctx* ctx, const cuapss_index* idx,
     CU_TRY(cudaMemsetAsync(ucnt, 0, sizeof(int) * std::max<size_t>(ns, 1), st));
     CU_TRY(cudaMemsetAsync(ccnt, 0, sizeof(unsigned long long) * std::max<size_t>(ns, 1), st));
     CU_TRY(cudaMemsetAsync(err, 0, sizeof(int), st));
+    // segment launches after the first start on the SMs the previous
+    // segment's CTAs leave (programmatic dependent launch; the segments
+    // write disjoint candidate regions and counters)
+    bool after_tiles = false;
     for (size_t s = 0; s < ns; ++s) {
       TileArgs& ta = tas[s];
       ta.unit_counter = ucnt + s;
@@ -539,8 +550,11 @@ cuapss_status cuapss::index_query_rows(cuapss_ctx* ctx, const cuapss_index* idx,
       ta.cand_sim = csim + coff[s];
       ta.cand_cap = cap[s];
       if (seg_tiles[s] == 0) continue;
-      if (idx->mixed) ST_TRY(launch_tiles_mma(ta, SQ.head16, segs[s]->head16, idx->p, grids[s], st));
-      else ST_TRY(launch_tiles_fp32(ta, grids[s], st));
+      if (idx->mixed)
+        ST_TRY(launch_tiles_mma(ta, SQ.head16, segs[s]->head16, idx->p, grids[s], st,
+                                after_tiles));
+      else ST_TRY(launch_tiles_fp32(ta, grids[s], st, after_tiles));
+      after_tiles = true;
     }
     int herr = 0;
     CU_TRY(cudaMemcpyAsync(hc.data(), ccnt, sizeof(unsigned long long) * std::max<size_t>(ns, 1),
@@ -562,6 +576,7 @@ cuapss_status cuapss::index_query_rows(cuapss_ctx* ctx, const cuapss_index* idx,
   int64_t ncand = 0;
   for (size_t s = 0; s < ns; ++s) ncand += (int64_t)hc[s];
   cudaEventRecord(ctx->ev[2], st);
+  nvtx.next("cuapss_index_query:finalize");
   // ---- finalize per segment, one sort
   uint64_t* okey = nullptr;
   uint32_t* oidx = nullptr;

@@ -90,6 +90,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_tiles_fp32(const TileArgs A) {
   }
   for (int i = tid; i < kBlockRows * kAccLd; i += kThreads) reinterpret_cast<int*>(S.acc)[i] = 0;
   __syncthreads();
+  allow_dependent_launch();
   uint32_t parity[2] = {0u, 0u};
   const int nchunks = A.p / kKC;
 
@@ -258,10 +259,20 @@ cuapss_status tiles_fp32_init() {
   return CUAPSS_OK;
 }
 
-cuapss_status launch_tiles_fp32(const TileArgs& a, int grid, cudaStream_t st) {
+cuapss_status launch_tiles_fp32(const TileArgs& a, int grid, cudaStream_t st, bool overlap_prev) {
   ST_TRY(tiles_fp32_init());
   if (a.p % kKC != 0) return CUAPSS_EINVAL;
-  k_tiles_fp32<<<grid, kThreads, kSmemBytes, st>>>(a);
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)grid);
+  cfg.blockDim = dim3(kThreads);
+  cfg.dynamicSmemBytes = kSmemBytes;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = overlap_prev ? 1 : 0;
+  CU_TRY(cudaLaunchKernelEx(&cfg, k_tiles_fp32, a));
   LAUNCH_CHECK();
   return CUAPSS_OK;
 }

@@ -234,6 +234,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_tiles_mma(const TileArgs A, con
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *S.tmem_base;
+  allow_dependent_launch();
 
   if (warp == 0) {
     // ------------------------------------------------------------ producer
@@ -500,18 +501,27 @@ cuapss_status tiles_mma_init() {
 }
 
 cuapss_status launch_tiles_mma(const TileArgs& a, const void* headI16, const void* headJ16,
-                               int p, int grid, cudaStream_t st) {
+                               int p, int grid, cudaStream_t st, bool overlap_prev) {
   ST_TRY(tiles_mma_init());
   if (p <= 0 || p % kKC != 0) return CUAPSS_EINVAL;
   MmaArgs m;
   m.headI16 = static_cast<const uint8_t*>(headI16);
   m.headJ16 = static_cast<const uint8_t*>(headJ16);
   m.nkc = p / kKC;
-  if (a.max_tailI <= kSmallCap)
-    k_tiles_mma<kSmallStages, kSmallCap>
-        <<<grid, kThreads, Cfg<kSmallStages, kSmallCap>::kSmem, st>>>(a, m);
-  else
-    k_tiles_mma<kBigStages, kBigCap><<<grid, kThreads, Cfg<kBigStages, kBigCap>::kSmem, st>>>(a, m);
+  const bool small = a.max_tailI <= kSmallCap;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)grid);
+  cfg.blockDim = dim3(kThreads);
+  cfg.dynamicSmemBytes =
+      small ? Cfg<kSmallStages, kSmallCap>::kSmem : Cfg<kBigStages, kBigCap>::kSmem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = overlap_prev ? 1 : 0;
+  if (small) CU_TRY(cudaLaunchKernelEx(&cfg, k_tiles_mma<kSmallStages, kSmallCap>, a, m));
+  else CU_TRY(cudaLaunchKernelEx(&cfg, k_tiles_mma<kBigStages, kBigCap>, a, m));
   LAUNCH_CHECK();
   return CUAPSS_OK;
 }

@@ -91,7 +91,11 @@ inline void order_units_for_l2(std::vector<int4>& units) {
 
 // Plain FP32 hybrid tile kernel (head: FP32 forward-list dot on TMA-staged
 // row tiles; tail: inverted-list scan into shared-memory accumulators).
-cuapss_status launch_tiles_fp32(const TileArgs& a, int grid, cudaStream_t st);
+// overlap_prev: the launch may start while the previous kernel on the
+// stream still runs (programmatic dependent launch), taking the SMs its
+// CTAs leave; only for work independent of that kernel's results.
+cuapss_status launch_tiles_fp32(const TileArgs& a, int grid, cudaStream_t st,
+                                bool overlap_prev = false);
 cuapss_status tiles_fp32_init();
 int tiles_fp32_max_grid();
 
@@ -99,7 +103,7 @@ int tiles_fp32_max_grid();
 // headI16 / headJ16: BF16 head blocks in the swizzled layout of
 // build_side; p a multiple of 64.
 cuapss_status launch_tiles_mma(const TileArgs& a, const void* headI16, const void* headJ16,
-                               int p, int grid, cudaStream_t st);
+                               int p, int grid, cudaStream_t st, bool overlap_prev = false);
 size_t tiles_mma_smem_bytes();
 cuapss_status tiles_mma_init();
 
