@@ -627,6 +627,17 @@ inline unsigned grid_for(int64_t work, int per_block) {
   return (unsigned)std::min<int64_t>(g, 148 * 32);
 }
 
+// Dynamic shared memory of the segment sorts of size class C (every class
+// above 48 KB needs the opt-in; it is set for all of them).
+template <int C>
+cuapss_status seg_sort_attr() {
+  constexpr int NT = kSegThr[C], E = kSegCap[C] / kSegThr[C];
+  const int sm = (int)seg_smem_bytes(NT, kSegCap[C]);
+  CU_TRY(cudaFuncSetAttribute(k_bil_seg<NT, E>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+  CU_TRY(cudaFuncSetAttribute(k_rec_seg<NT, E>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+  return CUAPSS_OK;
+}
+
 // Kernel attributes of the segment sorts (their shared memory), once per
 // device.
 cuapss_status seg_sort_init() {
@@ -636,11 +647,10 @@ cuapss_status seg_sort_init() {
   CU_TRY(cudaGetDevice(&dev));
   std::lock_guard<std::mutex> lk(mu);
   if (dev < 64 && ((done >> dev) & 1ull)) return CUAPSS_OK;
-  constexpr int C = kSegClasses - 1;
-  constexpr int NT = kSegThr[C], E = kSegCap[C] / kSegThr[C];
-  const int sm = (int)seg_smem_bytes(NT, kSegCap[C]);
-  CU_TRY(cudaFuncSetAttribute(k_bil_seg<NT, E>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
-  CU_TRY(cudaFuncSetAttribute(k_rec_seg<NT, E>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+  ST_TRY(seg_sort_attr<0>());
+  ST_TRY(seg_sort_attr<1>());
+  ST_TRY(seg_sort_attr<2>());
+  static_assert(kSegClasses == 3, "one attribute call per size class");
   if (dev < 64) done |= 1ull << dev;
   return CUAPSS_OK;
 }
