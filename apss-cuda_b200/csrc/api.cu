@@ -162,9 +162,11 @@ cuapss_status join_device(cuapss_ctx* ctx, const DevCsr& a, const DevCsr* b, flo
   if (mixed && p < 64) p = 64;
   PrepOptions po;
   po.p = p;
-  // Rows keep the caller's order: a 128-row block of random rows carries a
-  // near-average tail, so the tail's shared-memory staging fits almost every
-  // block (grouping long rows together would overflow it).
+  // Rows are dealt into 128-row blocks by their tail non-zeros, so every
+  // block's tail is near the mean: the tail's shared-memory staging fits
+  // every block (no chunked staging, the kernel variant with more operand
+  // stages) and the tiles' tail work is even. The finalize maps rows back.
+  po.balance_rows = 1;
   po.want_head32 = mixed ? 0 : 1;
   po.want_head16 = mixed ? 1 : 0;
   Side SA, SB;

@@ -189,6 +189,50 @@ __global__ void k_iota_i32(int32_t* v, int64_t n) {
     v[i] = (int32_t)i;
 }
 
+// Tail-balanced row blocks. One warp per caller row: its tail non-zeros
+// (features of rank >= p) into a sort key {count << rbits | row}.
+__global__ void k_row_tail_keys(const int64_t* __restrict__ rp, const int32_t* __restrict__ col,
+                                const int32_t* __restrict__ perm, int64_t n, int p, int rbits,
+                                uint64_t* __restrict__ keys, uint32_t* __restrict__ vals) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; i < n; i += warps) {
+    int cnt = 0;
+    for (int64_t e = rp[i] + lane; e < rp[i + 1]; e += 32) cnt += perm[col[e]] >= p ? 1 : 0;
+    cnt = warp_sum_i(cnt);
+    if (lane == 0) {
+      keys[i] = ((uint64_t)cnt << rbits) | (uint64_t)i;
+      vals[i] = (uint32_t)i;
+    }
+  }
+}
+
+// Places the rows, sorted by tail non-zeros ascending (sorted[k]), into row
+// blocks: the R = n - 128 F lightest rows fill the last, partial block; the
+// others are dealt to the F full blocks in snake order (round r gives block
+// b its (r F + b)-th row, or (r F + F - 1 - b)-th in odd rounds), so every
+// full block's tail is near the mean. rowperm[new] = caller row; newlen[new]
+// = its length.
+__global__ void k_deal_rows(const uint32_t* __restrict__ sorted, const int64_t* __restrict__ rp,
+                            int64_t n, int64_t F, int32_t* __restrict__ rowperm,
+                            int64_t* __restrict__ newlen) {
+  const int64_t R = n - F * kBlockRows;
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n;
+       k += (int64_t)gridDim.x * blockDim.x) {
+    int64_t pos;
+    if (k < R) {
+      pos = F * kBlockRows + k;
+    } else {
+      const int64_t kk = k - R, r = kk / F, q = kk % F;
+      const int64_t blk = (r & 1) ? F - 1 - q : q;
+      pos = blk * kBlockRows + r;
+    }
+    const uint32_t old = sorted[k];
+    rowperm[pos] = (int32_t)old;
+    newlen[pos] = rp[old + 1] - rp[old];
+  }
+}
+
 // One warp per row, one pass over the caller's CSR: feature ids remapped to
 // their frequency rank; the head entries (rank < p) scattered straight into
 // the dense head block (BF16 tiles in the tensor core's swizzled layout,
@@ -207,7 +251,9 @@ __global__ void k_iota_i32(int32_t* v, int64_t n) {
 // in shared memory ready for tcgen05.mma. FP32 layout: head32[b][f][rr].
 __global__ void k_split_rows(const int64_t* __restrict__ rp, const int32_t* __restrict__ col,
                              const float* __restrict__ val, const int32_t* __restrict__ perm,
-                             int64_t n, int p, int32_t* __restrict__ col2,
+                             const int32_t* __restrict__ rowperm,
+                             const int64_t* __restrict__ rp_out, int64_t n, int p,
+                             int32_t* __restrict__ col2,
                              float* __restrict__ val2, int32_t* __restrict__ hlen,
                              int32_t* __restrict__ nnz_row, float* __restrict__ hnorm,
                              int64_t* __restrict__ tcount, int32_t* __restrict__ blk_maxnnz,
@@ -217,7 +263,9 @@ __global__ void k_split_rows(const int64_t* __restrict__ rp, const int32_t* __re
   const unsigned lt = (1u << lane) - 1u;
   const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
   for (int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; i < n; i += warps) {
-    const int64_t lo = rp[i], hi = rp[i + 1];
+    const int64_t src = rowperm ? (int64_t)rowperm[i] : i;  // the caller's row at place i
+    const int64_t lo = rp[src], hi = rp[src + 1];
+    const int64_t ohi = rp_out[i + 1];  // this row's range in col2/val2 ends here
     const int64_t b = i / kBlockRows, rr = i % kBlockRows;
     int64_t nh = 0, nt = 0;
     double hs = 0.0;
@@ -238,7 +286,7 @@ __global__ void k_split_rows(const int64_t* __restrict__ rp, const int32_t* __re
         }
         if (head32) head32[(b * p + rank) * kBlockRows + rr] = v;
       } else if (valid) {
-        const int64_t dst = hi - 1 - (nt + __popc(tb & lt));
+        const int64_t dst = ohi - 1 - (nt + __popc(tb & lt));
         col2[dst] = rank;
         val2[dst] = v;
       }
@@ -795,12 +843,37 @@ cuapss_status build_side(Side& s, const PrepOptions& o, const int32_t* perm, Wor
   const uint64_t fmask = (fbits >= 64) ? ~0ull : ((1ull << fbits) - 1);
   const uint64_t rmask = (1ull << rbits) - 1;
   const std::string t = tag + ":";
-  // ---- rows keep the caller's order: identity row map, rp2 = rp0 ----
+  // ---- row order: the caller's, or tail-balanced blocks ----
   ST_TRY(ws.get(t + "rowperm", (size_t)n, &s.rowperm));
-  k_iota_i32<<<grid_for(n, kThreads), kThreads, 0, st>>>(s.rowperm, n);
-  LAUNCH_CHECK();
   ST_TRY(ws.get(t + "rp2", (size_t)n + 1, &s.rp2));
-  CU_TRY(cudaMemcpyAsync(s.rp2, s.rp0, sizeof(int64_t) * (n + 1), cudaMemcpyDeviceToDevice, st));
+  const int32_t* place = nullptr;  // new row -> caller row, null: identity
+  const int64_t full_blocks = n / kBlockRows;
+  if (o.balance_rows && full_blocks >= 2) {
+    const int rbits = std::max(1, bits_for((uint64_t)n));
+    uint64_t* keys = nullptr;
+    uint32_t* vals = nullptr;
+    int64_t* newlen = nullptr;
+    ST_TRY(ws.get(t + "bal:keys", (size_t)n, &keys));
+    ST_TRY(ws.get(t + "bal:vals", (size_t)n, &vals));
+    ST_TRY(ws.get(t + "bal:len", (size_t)n + 1, &newlen));
+    k_row_tail_keys<<<grid_for(n * 32, kThreads), kThreads, 0, st>>>(s.rp0, s.col0, perm, n, p,
+                                                                     rbits, keys, vals);
+    LAUNCH_CHECK();
+    // tail counts are < 2^31: rbits + 31 key bits at most (the sort takes the
+    // bits of the largest possible count, bounded by d)
+    ST_TRY(radix_sort_pairs(keys, vals, n, rbits + std::max(1, bits_for((uint64_t)d)), ws,
+                            t + "bal", st));
+    k_deal_rows<<<grid_for(n, kThreads), kThreads, 0, st>>>(vals, s.rp0, n, full_blocks,
+                                                            s.rowperm, newlen);
+    LAUNCH_CHECK();
+    ST_TRY(exclusive_scan<int64_t>(newlen, s.rp2, n, s.rp2 + n, ws, t + "bal:scan", st));
+    place = s.rowperm;
+  } else {
+    k_iota_i32<<<grid_for(n, kThreads), kThreads, 0, st>>>(s.rowperm, n);
+    LAUNCH_CHECK();
+    CU_TRY(cudaMemcpyAsync(s.rp2, s.rp0, sizeof(int64_t) * (n + 1), cudaMemcpyDeviceToDevice,
+                           st));
+  }
   // ---- one pass: remap, head block, row statistics, tail suffixes ----
   ST_TRY(ws.get(t + "col2", (size_t)std::max<int64_t>(nnz, 1), &s.col2));
   ST_TRY(ws.get(t + "val2", (size_t)std::max<int64_t>(nnz, 1), &s.val2));
@@ -827,8 +900,8 @@ cuapss_status build_side(Side& s, const PrepOptions& o, const int32_t* perm, Wor
     CU_TRY(cudaMemsetAsync(s.head16, 0, hb * sizeof(__nv_bfloat16), st));
   }
   k_split_rows<<<grid_for(n * 32, kThreads), kThreads, 0, st>>>(
-      s.rp0, s.col0, s.val0, perm, n, p, s.col2, s.val2, s.hlen, s.nnz_row, s.hnorm, tcount,
-      s.blk_maxnnz, s.head16, nkc, s.head32);
+      s.rp0, s.col0, s.val0, perm, place, s.rp2, n, p, s.col2, s.val2, s.hlen, s.nnz_row,
+      s.hnorm, tcount, s.blk_maxnnz, s.head16, nkc, s.head32);
   LAUNCH_CHECK();
   ST_TRY(ws.get(t + "tptr", (size_t)n + 1, &s.tptr));
   ST_TRY(exclusive_scan<int64_t>(tcount, s.tptr, n, s.tptr + n, ws, t + "tptr", st));

@@ -15,6 +15,7 @@ struct PrepOptions {
   int want_head32 = 1;  // build the FP32 head block
   int want_head16 = 0;  // build the BF16 head block
   int want_csc = 0;     // build the global inverted lists (cptr/csc)
+  int balance_rows = 0; // deal rows into blocks by tail non-zeros (rowperm); else caller order
 };
 
 // Validates a device CSR. counts (device, d entries, may be null) are
