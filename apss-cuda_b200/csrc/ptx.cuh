@@ -169,6 +169,10 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
+// 32 lanes x 16 or 32 consecutive columns, by the array's length.
+__device__ __forceinline__ void tmem_ld(uint32_t taddr, uint32_t (&v)[16]) { tmem_ld16(taddr, v); }
+__device__ __forceinline__ void tmem_ld(uint32_t taddr, uint32_t (&v)[32]) { tmem_ld32(taddr, v); }
+
 // Shared-memory matrix descriptor: K-major operand, 128-byte swizzle,
 // 8-row core groups 1024 bytes apart (SBO), version 1 (tcgen05).
 __device__ __forceinline__ uint64_t umma_desc_sw128(const void* smem) {

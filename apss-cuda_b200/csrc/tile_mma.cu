@@ -11,7 +11,9 @@
 // per-pair sparse-dense head dot (similarity_apss_rest / similarity_join_rest,
 // fengyilin118/APSS-CUDA similarity_search.cu:441-506, 854-915).
 //
-// Warp roles (one CTA per SM, persistent over a static share of the units):
+// Warp roles (one CTA per SM, persistent; the producer takes units of work
+// from a global counter as the CTA gets to them and publishes their ids to
+// the other roles through a ring of kUnitRing slots):
 //   warp 0          producer: bulk copies of I and J operand tiles into a
 //                   3- or 4-stage shared-memory ring (mbarrier full/empty);
 //   warp 1          MMA: allocates 256 tensor-memory columns (two 128-column
@@ -65,11 +67,14 @@ constexpr int kTileBytes = kBlockRows * kKC * 2;  // 16 KB per operand chunk
 constexpr int kSlabCols = kJSegRows;          // tile columns per slab (one J segment)
 constexpr int kSlabs = kJSegs;                // slabs per tile
 constexpr int kSlabInts = kBlockRows * kSlabCols;  // one slab accumulator
-constexpr int kEpiCols = kSlabCols / (kEW / 4);    // slab columns per epilogue thread (16)
+constexpr int kEpiCols = kSlabCols / (kEW / 4);    // slab columns per epilogue thread
+static_assert(kEpiCols == 16 || kEpiCols == 32, "tensor-memory loads of 16 or 32 columns");
 constexpr uint32_t kTmemCols = 256;
 constexpr int kTailBar = 1;
 constexpr int kEpiBar = 2;
-constexpr int kBatch = 4;                     // J postings per thread per load batch
+constexpr int kBatch = 3;                     // J postings per thread per load batch
+constexpr int kUnitRing = 8;                  // unit ids published ahead by the producer
+constexpr int kUnitReaders = 1 + kTW + kEW;   // MMA thread + tail warps + epilogue warps
 static_assert(kSlabCols == 32, "slab accumulator rows are 32 ints (8 swizzled groups)");
 
 struct SmemM {
@@ -83,6 +88,9 @@ struct SmemM {
   uint64_t* afull;
   uint64_t* aempty;
   uint64_t* drain;
+  uint64_t* ufull;      // [kUnitRing] a unit id was published
+  uint64_t* uempty;     // [kUnitRing] every role has read it
+  int* uring;           // [kUnitRing] unit ids
   uint32_t* tmem_base;
   int* abort;
   TailStage ts;
@@ -94,11 +102,12 @@ __host__ __device__ constexpr size_t align_up(size_t x, size_t a) { return (x + 
 // staged tail postings.
 template <int STAGES, int CAP>
 struct Cfg {
-  static constexpr int kBars = 2 * STAGES + 2 + 2 + 2 + 2 + 1;
+  static constexpr int kBars = 2 * STAGES + 2 + 2 + 2 + 2 + 1 + 2 * kUnitRing;
   static constexpr size_t kAcc = (size_t)STAGES * 2 * kTileBytes;
   static constexpr size_t kHnj = align_up(kAcc + (size_t)2 * kSlabInts * 4, 16);
   static constexpr size_t kBar = align_up(kHnj + (size_t)2 * kBlockRows * 4, 16);
-  static constexpr size_t kTmem = align_up(kBar + (size_t)kBars * 8, 16);
+  static constexpr size_t kRing = align_up(kBar + (size_t)kBars * 8, 16);
+  static constexpr size_t kTmem = align_up(kRing + (size_t)kUnitRing * 4, 16);
   static constexpr size_t kAbort = kTmem + 16;
   static constexpr size_t kTail = align_up(kAbort + 16, 16);
   static constexpr size_t kTotal = align_up(kTail + tail_stage_bytes<CAP>(), 16);
@@ -122,6 +131,9 @@ __device__ __forceinline__ SmemM carve(uint8_t* raw) {
   s.afull = b + 2 * STAGES + 4;
   s.aempty = b + 2 * STAGES + 6;
   s.drain = b + 2 * STAGES + 8;
+  s.ufull = b + 2 * STAGES + 9;
+  s.uempty = b + 2 * STAGES + 9 + kUnitRing;
+  s.uring = reinterpret_cast<int*>(base + C::kRing);
   s.tmem_base = reinterpret_cast<uint32_t*>(base + C::kTmem);
   s.abort = reinterpret_cast<int*>(base + C::kAbort);
   s.ts = tail_stage_at<CAP>(base + C::kTail);
@@ -221,6 +233,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_tiles_mma(const TileArgs A, con
       mbar_init(&S.aempty[b], kEW);
     }
     mbar_init(S.drain, 1);
+    for (int k = 0; k < kUnitRing; ++k) {
+      mbar_init(&S.ufull[k], 1);
+      mbar_init(&S.uempty[k], kUnitReaders);
+    }
     *abort = 0;
     fence_mbar_init();
   }
@@ -239,9 +255,20 @@ __global__ void __launch_bounds__(kThreads, 1) k_tiles_mma(const TileArgs A, con
   if (warp == 0) {
     // ------------------------------------------------------------ producer
     if (lane == 0) {
+      // units are taken from a global counter as the CTA gets to them and
+      // published to the other roles through the unit ring
       uint32_t it = 0;
       bool ok = true;
-      for (int u = blockIdx.x; ok && u < A.nunits; u += gridDim.x) {
+      for (uint32_t k = 0; ok; ++k) {
+        const uint32_t slot = k % kUnitRing, ur = k / kUnitRing;
+        if (!wait_or_abort(&S.uempty[slot], (ur & 1u) ^ 1u, abort)) {
+          raise_abort(A, abort);
+          break;
+        }
+        const int u = atomicAdd(A.unit_counter, 1);
+        reinterpret_cast<volatile int*>(S.uring)[slot] = u;
+        mbar_arrive(&S.ufull[slot]);
+        if (u >= A.nunits) break;
         const int4 U = A.units[u];
         if (U.y >= U.z) continue;
         for (int J = U.y; ok && J < U.z; ++J) {
@@ -273,7 +300,15 @@ __global__ void __launch_bounds__(kThreads, 1) k_tiles_mma(const TileArgs A, con
       const uint32_t idesc = umma_idesc_bf16(kBlockRows, kBlockRows);
       uint32_t it = 0, tt = 0;
       bool ok = true;
-      for (int u = blockIdx.x; ok && u < A.nunits; u += gridDim.x) {
+      for (uint32_t k = 0; ok; ++k) {
+        const uint32_t slot = k % kUnitRing, ur = k / kUnitRing;
+        if (!wait_or_abort(&S.ufull[slot], ur & 1u, abort)) {
+          raise_abort(A, abort);
+          break;
+        }
+        const int u = reinterpret_cast<volatile int*>(S.uring)[slot];
+        mbar_arrive(&S.uempty[slot]);
+        if (u >= A.nunits) break;
         const int4 U = A.units[u];
         if (U.y >= U.z) continue;
         for (int J = U.y; ok && J < U.z; ++J, ++tt) {
@@ -316,31 +351,45 @@ __global__ void __launch_bounds__(kThreads, 1) k_tiles_mma(const TileArgs A, con
     // Each thread keeps the first batch of the next slab's J postings in
     // registers (loaded while it works on this slab), so the load latency
     // of a slab's records overlaps the previous slab's probes.
+    // The J segment pointers of the next J block are loaded one block ahead
+    // (32-bit: a side holds fewer than 2^32 tail postings).
     const int ttid = threadIdx.x - 64;
     bool live = true;
     uint32_t g = 0;  // slabs processed by this CTA
-    for (int u = blockIdx.x; u < A.nunits; u += gridDim.x) {
+    for (uint32_t ku = 0;; ++ku) {
+      const uint32_t slot = ku % kUnitRing, ur = ku / kUnitRing;
+      live = warp_wait(A, &S.ufull[slot], ur & 1u, abort, live);
+      const int u = live ? reinterpret_cast<volatile int*>(S.uring)[slot] : A.nunits;
+      __syncwarp();
+      if (live && lane == 0) mbar_arrive(&S.uempty[slot]);
+      // every tail warp is done with the previous unit's staging; all stop together
+      if (named_bar_or(kTailBar, kTT, u >= A.nunits)) break;
       const int4 U = A.units[u];
       if (U.y >= U.z) continue;
       const int I = U.x;
-      named_bar(kTailBar, kTT);  // every tail warp is done with the previous unit's staging
       const int nch = tail_nchunks<CAP>(A, I);
       TailI T{};
       if (nch == 1) T = stage_tail_chunk<kTT, kTailBar, CAP>(A, S.ts, I, 0, ttid);
+      uint32_t hc[kJSegs + 1], hn[kJSegs + 1];
+#pragma unroll
+      for (int m = 0; m <= kJSegs; ++m) hc[m] = (uint32_t)A.hptrJ[kJSegs * U.y + m];
       uint2 nxt[kBatch];
-      load_batch<kBatch>(A, A.hptrJ[kJSegs * U.y], A.hptrJ[kJSegs * U.y + 1], ttid, kTT, nxt);
+      load_batch<kBatch>(A, hc[0], hc[1], ttid, kTT, nxt);
       for (int J = U.y; J < U.z; ++J) {
+        if (J + 1 < U.z) {
+#pragma unroll
+          for (int m = 0; m <= kJSegs; ++m) hn[m] = (uint32_t)A.hptrJ[kJSegs * (J + 1) + m];
+        }
+#pragma unroll
         for (int q = 0; q < kSlabs; ++q, ++g) {
           const uint32_t k = g & 1u, use = g >> 1;
-          const int64_t k0 = A.hptrJ[kJSegs * J + q], k1 = A.hptrJ[kJSegs * J + q + 1];
+          const int64_t k0 = hc[q], k1 = hc[q + 1];
           uint2 cur[kBatch];
 #pragma unroll
           for (int b = 0; b < kBatch; ++b) cur[b] = nxt[b];
           // the next slab of this unit: its first batch, in flight from here
-          const int qn = q + 1 < kSlabs ? q + 1 : 0, Jn = q + 1 < kSlabs ? J : J + 1;
-          if (Jn < U.z)
-            load_batch<kBatch>(A, A.hptrJ[kJSegs * Jn + qn], A.hptrJ[kJSegs * Jn + qn + 1], ttid,
-                               kTT, nxt);
+          if (q + 1 < kSlabs) load_batch<kBatch>(A, hc[q + 1], hc[q + 2], ttid, kTT, nxt);
+          else if (J + 1 < U.z) load_batch<kBatch>(A, hn[0], hn[1], ttid, kTT, nxt);
           live = warp_wait(A, &S.aempty[k], (use & 1u) ^ 1u, abort, live);
           int* acc = S.acc + k * kSlabInts;
           const int cofs = q * kSlabCols;
@@ -362,6 +411,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_tiles_mma(const TileArgs A, con
           __syncwarp();
           if (live && lane == 0) mbar_arrive(&S.afull[k]);
         }
+#pragma unroll
+        for (int m = 0; m <= kJSegs; ++m) hc[m] = hn[m];
       }
     }
   } else {
@@ -373,7 +424,13 @@ __global__ void __launch_bounds__(kThreads, 1) k_tiles_mma(const TileArgs A, con
     const int row = 32 * q4 + lane;  // tile row of this thread
     bool live = true;
     uint32_t tt = 0, g = 0;
-    for (int u = blockIdx.x; u < A.nunits; u += gridDim.x) {
+    for (uint32_t ku = 0;; ++ku) {
+      const uint32_t slot = ku % kUnitRing, ur = ku / kUnitRing;
+      live = warp_wait(A, &S.ufull[slot], ur & 1u, abort, live);
+      const int u = live ? reinterpret_cast<volatile int*>(S.uring)[slot] : A.nunits;
+      __syncwarp();
+      if (live && lane == 0) mbar_arrive(&S.uempty[slot]);
+      if (named_bar_or(kEpiBar, kET, u >= A.nunits)) break;  // all stop together
       const int4 U = A.units[u];
       if (U.y >= U.z) continue;
       const int I = U.x;
@@ -404,9 +461,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_tiles_mma(const TileArgs A, con
             // ---- head (tensor memory) + tail (slab accumulator) vs t - eps
             const int cbase = q * kSlabCols + colh * kEpiCols;  // first tile column
             uint32_t v[kEpiCols];
-            tmem_ld16(tmem + b * (uint32_t)kBlockRows + (uint32_t)cbase +
-                          ((uint32_t)(32 * q4) << 16),
-                      v);
+            const uint32_t taddr =
+                tmem + b * (uint32_t)kBlockRows + (uint32_t)cbase + ((uint32_t)(32 * q4) << 16);
+            tmem_ld(taddr, v);
             int* arow = S.acc + k * kSlabInts + row * kSlabCols;
             const float4* hn4 = reinterpret_cast<const float4*>(hnj + cbase);
             uint32_t pass = 0;
