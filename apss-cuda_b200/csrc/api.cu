@@ -40,15 +40,19 @@ void record_cuda_error(cudaError_t e, const char* what, const char* file, int li
 const char* last_error_message() { return g_last_error; }
 
 // Per-tile cost model of the mixed-precision tile kernel, whose tensor-core
-// side and sparse-tail side overlap, so the slower one sets the pace:
+// side and sparse-tail side mostly overlap, so the slower one sets the pace:
 //   head  kHeadChunkNs per 64 head features (operand stream and MMAs of a
 //         128 x 128 tile),
 //   tail  kTailPostingNs per tail posting of the J block (one probe of the
-//         staged I postings); a block holds 128 x (tail non-zeros per row).
-// The head width p minimises max(head, tail) over multiples of 64; the tail
-// non-zeros at each p come from the posting counts in frequency order.
-constexpr double kHeadChunkNs = 440.0;
-constexpr double kTailPostingNs = 1.04;
+//         staged I postings); a block holds 128 x (tail non-zeros per row),
+//   cost  max(head, tail) + kOverlapLoss x min(head, tail).
+// Fitted to tile-kernel times on the n = d = 1M workload's shape at 200,000
+// rows for p = 768 .. 2048. The head width p minimises the cost over
+// multiples of 64; the tail non-zeros at each p come from the posting counts
+// in frequency order.
+constexpr double kHeadChunkNs = 388.0;
+constexpr double kTailPostingNs = 1.6;
+constexpr double kOverlapLoss = 0.06;
 constexpr int kMaxModelHead = 8192;
 
 int choose_head_width(int precision, int64_t n, int64_t d, int64_t nnz,
@@ -65,7 +69,7 @@ int choose_head_width(int precision, int64_t n, int64_t d, int64_t nnz,
     const double tail_per_row = (double)(nnz - prefix[(size_t)p]) / (double)n;
     const double head = kHeadChunkNs * (double)(p / 64);
     const double tail = kTailPostingNs * kBlockRows * tail_per_row;
-    const double cost = std::max(head, tail);
+    const double cost = std::max(head, tail) + kOverlapLoss * std::min(head, tail);
     if (cost < best - 1e-9) {
       best = cost;
       best_p = (int)p;
@@ -166,7 +170,9 @@ cuapss_status join_device(cuapss_ctx* ctx, const DevCsr& a, const DevCsr* b, flo
   // block's tail is near the mean: the tail's shared-memory staging fits
   // every block (no chunked staging, the kernel variant with more operand
   // stages) and the tiles' tail work is even. The finalize maps rows back.
-  po.balance_rows = 1;
+  // (a sharded run keeps the caller's order: shard s owns the caller-row
+  // blocks b with b % nshards == s, which cuapss_shard_blocks lists)
+  po.balance_rows = nshards == 1 ? 1 : 0;
   po.want_head32 = mixed ? 0 : 1;
   po.want_head16 = mixed ? 1 : 0;
   Side SA, SB;
@@ -219,8 +225,8 @@ cuapss_status join_device(cuapss_ctx* ctx, const DevCsr& a, const DevCsr* b, flo
   if (d - SA.p > (int64_t)(1u << 20) - 2) return CUAPSS_EINVAL;  // 20-bit tail feature keys
   set_tile_margins(ta, nrm2, mixed);
   // ---- units: I block x J range; an I block's J range is cut into chunks
-  // of about equal cost (about 16 units per CTA), heavier blocks get shorter
-  // ranges. CTAs take units round-robin (mixed kernel) or from a counter.
+  // of about equal cost, heavier blocks get shorter ranges. CTAs take units
+  // from a counter as they get to them.
   const int grid_max = ctx->sms;
   std::vector<int4> units;
   {
@@ -231,7 +237,9 @@ cuapss_status join_device(cuapss_ctx* ctx, const DevCsr& a, const DevCsr* b, flo
     // a shard takes the I blocks with I mod nshards == shard
     double total = 0.0;
     for (int I = shard; I < SA.nb; I += nshards) total += weight(I) * (SJ->nb - (self ? I : 0));
-    const double target = std::max(1.0, total / (grid_max * 16.0));
+    // about 64 units per CTA: the CTAs take them dynamically, so the last
+    // ones to finish wait at most a short unit
+    const double target = std::max(1.0, total / (grid_max * 64.0));
     for (int I = shard; I < SA.nb; I += nshards) {
       const int jb = self ? I : 0, je = SJ->nb;
       const int chunk = (int)std::max(1.0, std::floor(target / weight(I)));

@@ -317,10 +317,12 @@ def tile_roofline(stats, p, pairs, n, world, prec_mixed, x, peaks_):
         head_flops *= s0["tiles"] / (nb * (nb + 1) / 2)
     if prec_mixed:
         achieved = head_flops / (tile_ms / 1e3) / 1e12
-        tr = TILE_TRAFFIC_PER_TILE.get(p)
+        traffic = TILE_TRAFFIC_PER_CHUNK * s0["tiles"] * (p // 64)
         return {"bound": "tensor", "achieved": achieved, "peak": bf16_sus, "unit": "TFLOP/s",
                 "frac": achieved / bf16_sus,
-                "traffic": tr * s0["tiles"] if tr else None,
+                "traffic": traffic,
+                "traffic_source": "ncu launch list at 200,000 rows of this shape, scaled by "
+                                  "tiles x p / 64 (profiles/launches_mixed1m_n200k_dram.md)",
                 "peak_source": f"{src} (sustained BF16: the kernel runs for about a second "
                                f"inside a multi-second step)",
                 "frac_of_burst": achieved / bf16,
@@ -337,10 +339,12 @@ def tile_roofline(stats, p, pairs, n, world, prec_mixed, x, peaks_):
                     f"{head_flops / (tile_ms / 1e3) / 1e12:.1f} TFLOP/s"}
 
 
-# DRAM bytes (read + write) of one k_tiles_mma launch per 128 x 128 tile, from
-# ncu captures of the mixed_1m shape at 200,000 rows (the full-size launch is
-# too large to capture); traffic grows with the tiles processed.
-TILE_TRAFFIC_PER_TILE = {}
+# DRAM bytes (read + write) of k_tiles_mma per 128 x 128 tile and 64 head
+# features, from the ncu launch list of the n = d = 1M workload's shape at
+# 200,000 rows (137.0 GB over 1,222,266 tiles at p = 960; the full-size launch
+# is too large to capture). Scaled by tiles x p / 64; at full size the head
+# block is a larger multiple of the L2, so the true figure is higher.
+TILE_TRAFFIC_PER_CHUNK = 137.0e9 / 1_222_266 / 15
 
 
 def dry_shards(args, rank, world):
@@ -895,7 +899,7 @@ def run_serve(args, rank, world, local):
                 srv.wait(tk, capacity=1 << 20)
             sweep = []
             with Clocks(local) as clk:
-                for factor in (0.5, 1.0, 2.0, 4.0):
+                for factor in (0.5, 0.75, 1.0, 2.0):
                     reqs = [("query",) + queries(256) for _ in range(args.serve_requests)]
                     rate = factor * 1000.0 / lone_ms
                     infos, wall = drive(srv, reqs, rate)
