@@ -50,6 +50,10 @@ const char* last_error_message() { return g_last_error; }
 // rows for p = 768 .. 2048. The head width p minimises the cost over
 // multiples of 64; the tail non-zeros at each p come from the posting counts
 // in frequency order.
+// Explicit rare-feature pairs of one self-join (12 bytes each, twice for the
+// sort): at most 400M.
+constexpr int64_t kMaxExplicitPairs = 400000000;
+
 constexpr double kHeadChunkNs = 388.0;
 constexpr double kTailPostingNs = 1.6;
 constexpr double kOverlapLoss = 0.06;
@@ -175,6 +179,12 @@ cuapss_status join_device(cuapss_ctx* ctx, const DevCsr& a, const DevCsr* b, flo
   po.balance_rows = nshards == 1 ? 1 : 0;
   po.want_head32 = mixed ? 0 : 1;
   po.want_head16 = mixed ? 1 : 0;
+  // Tail features that occur in at most a few rows are paired explicitly
+  // (self-joins on one shard): probing their postings in every tile is
+  // almost all misses.
+  if (self && nshards == 1)
+    ST_TRY(choose_rare_features(counts, perm, d, p, kMaxExplicitPairs, ws, st, &po.rare_from,
+                                &po.rare_max_count));
   Side SA, SB;
   SA.rp0 = a.rp;
   SA.col0 = a.col;
@@ -218,6 +228,11 @@ cuapss_status join_device(cuapss_ctx* ctx, const DevCsr& a, const DevCsr* b, flo
   ta.hnormJ = SJ->hnorm;
   ta.hptrJ = SJ->hptr;
   ta.bilJ_rec = SJ->bil_rec;
+  if (self && SA.n_explicit > 0) {
+    ta.ex_off = SA.ex_off;
+    ta.ex_key = SA.ex_key;
+    ta.ex_val = SA.ex_val;
+  }
   ta.p = SA.p;
   ta.self = self ? 1 : 0;
   ta.t = t;

@@ -23,6 +23,7 @@
 
 #include "prep.cuh"
 #include "prims.cuh"
+#include "tail.cuh"
 
 namespace cuapss {
 
@@ -233,6 +234,10 @@ __global__ void k_deal_rows(const uint32_t* __restrict__ sorted, const int64_t* 
   }
 }
 
+// Entries of rank >= rare_from (features that occur in few rows) are neither
+// head nor tail: they go, remapped, to the front of the row's range (a
+// prefix of length rcount[r]) and their pairs are enumerated explicitly.
+//
 // One warp per row, one pass over the caller's CSR: feature ids remapped to
 // their frequency rank; the head entries (rank < p) scattered straight into
 // the dense head block (BF16 tiles in the tensor core's swizzled layout,
@@ -258,16 +263,17 @@ __global__ void k_split_rows(const int64_t* __restrict__ rp, const int32_t* __re
                              int32_t* __restrict__ nnz_row, float* __restrict__ hnorm,
                              int64_t* __restrict__ tcount, int32_t* __restrict__ blk_maxnnz,
                              __nv_bfloat16* __restrict__ head16, int nkc,
-                             float* __restrict__ head32) {
+                             float* __restrict__ head32, int64_t rare_from,
+                             int64_t* __restrict__ rcount) {
   const int lane = threadIdx.x & 31;
   const unsigned lt = (1u << lane) - 1u;
   const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
   for (int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; i < n; i += warps) {
     const int64_t src = rowperm ? (int64_t)rowperm[i] : i;  // the caller's row at place i
     const int64_t lo = rp[src], hi = rp[src + 1];
-    const int64_t ohi = rp_out[i + 1];  // this row's range in col2/val2 ends here
+    const int64_t olo = rp_out[i], ohi = rp_out[i + 1];  // this row's range in col2/val2
     const int64_t b = i / kBlockRows, rr = i % kBlockRows;
-    int64_t nh = 0, nt = 0;
+    int64_t nh = 0, nt = 0, nr = 0;
     double hs = 0.0;
     for (int64_t base = lo; base < hi; base += 32) {
       const int64_t e = base + lane;
@@ -275,7 +281,9 @@ __global__ void k_split_rows(const int64_t* __restrict__ rp, const int32_t* __re
       const int32_t rank = valid ? perm[col[e]] : 0;
       const float v = valid ? val[e] : 0.0f;
       const bool head = valid && rank < p;
-      const unsigned tb = __ballot_sync(0xffffffffu, valid && !head);
+      const bool rare = valid && (int64_t)rank >= rare_from;
+      const unsigned tb = __ballot_sync(0xffffffffu, valid && !head && !rare);
+      const unsigned rb = __ballot_sync(0xffffffffu, rare);
       if (head) {
         hs += (double)v * (double)v;
         if (head16) {
@@ -285,6 +293,10 @@ __global__ void k_split_rows(const int64_t* __restrict__ rp, const int32_t* __re
           head16[off] = __float2bfloat16_rn(v);
         }
         if (head32) head32[(b * p + rank) * kBlockRows + rr] = v;
+      } else if (rare) {
+        const int64_t dst = olo + nr + __popc(rb & lt);
+        col2[dst] = rank;
+        val2[dst] = v;
       } else if (valid) {
         const int64_t dst = ohi - 1 - (nt + __popc(tb & lt));
         col2[dst] = rank;
@@ -292,6 +304,7 @@ __global__ void k_split_rows(const int64_t* __restrict__ rp, const int32_t* __re
       }
       nh += __popc(__ballot_sync(0xffffffffu, head));
       nt += __popc(tb);
+      nr += __popc(rb);
     }
     hs = warp_sum_d(hs);
     if (lane == 0) {
@@ -299,6 +312,7 @@ __global__ void k_split_rows(const int64_t* __restrict__ rp, const int32_t* __re
       nnz_row[i] = (int32_t)(hi - lo);
       hnorm[i] = __double2float_ru(sqrt(hs));
       tcount[i] = nt;
+      if (rcount) rcount[i] = nr;
       atomicMax(&blk_maxnnz[b], (int32_t)(hi - lo));
     }
   }
@@ -336,7 +350,8 @@ __global__ void k_tail_entries(const int64_t* __restrict__ rp2, const int32_t* _
   const int lane = threadIdx.x & 31;
   const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
   for (int64_t r = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; r < n; r += warps) {
-    const int64_t lo = rp2[r] + hlen[r], hi = rp2[r + 1];
+    // the tail entries are the suffix of the row's range (tptr counts them)
+    const int64_t hi = rp2[r + 1], lo = hi - (tptr[r + 1] - tptr[r]);
     const int64_t t0 = tptr[r];
     const uint64_t blk = (uint64_t)(r / kBlockRows);
     const uint64_t hblk = (uint64_t)(r / kJSegRows);
@@ -725,6 +740,140 @@ cuapss_status launch_seg_sorts(const int32_t* idsB, const int (&fB)[kSegClasses 
   return CUAPSS_OK;
 }
 
+// ---- explicit pairs of rare features ----
+// A feature that occurs in at most a few rows is a waste to probe: its J
+// postings meet the I blocks' staged lists of almost every tile for nothing.
+// Its pairs are enumerated instead: the rare entries are sorted by (feature,
+// row), every pair of postings of one feature gives a record {triangular
+// tile index << 14 | row in I block << 7 | column in J block} with the
+// fixed-point product, and the records are sorted by tile, so that a tile
+// adds its few records to its tail accumulator directly.
+
+// One warp per row: its rare entries (the row's prefix) as sort keys
+// {rare feature << rbits | row} with the value bits.
+__global__ void k_rare_keys(const int64_t* __restrict__ rp2, const int32_t* __restrict__ col2,
+                            const float* __restrict__ val2, const int64_t* __restrict__ rptr,
+                            int64_t n, int64_t rare_from, int rbits, uint64_t* __restrict__ keys,
+                            uint32_t* __restrict__ vals) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t r = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; r < n; r += warps) {
+    const int64_t o = rptr[r], m = rptr[r + 1] - o, lo = rp2[r];
+    for (int64_t k = lane; k < m; k += 32) {
+      keys[o + k] = ((uint64_t)(col2[lo + k] - rare_from) << rbits) | (uint64_t)r;
+      vals[o + k] = __float_as_uint(val2[lo + k]);
+    }
+  }
+}
+
+// Pairs that posting k of the sorted rare list opens: the later postings of
+// its feature (a feature has at most max_run postings).
+__global__ void k_rare_pair_counts(const uint64_t* __restrict__ keys, int64_t m, int rbits,
+                                   int max_run, int64_t* __restrict__ cnt) {
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < m;
+       k += (int64_t)gridDim.x * blockDim.x) {
+    const uint64_t f = keys[k] >> rbits;
+    int64_t e = k + 1;
+    while (e < m && e - k <= max_run && (keys[e] >> rbits) == f) ++e;
+    cnt[k] = e - k - 1;
+  }
+}
+
+__device__ __forceinline__ uint64_t tri_tile(int64_t I, int64_t J, int64_t nb) {
+  return (uint64_t)(I * nb - I * (I - 1) / 2 + (J - I));
+}
+
+// The records of the pairs posting k opens, at off[k].
+__global__ void k_rare_pairs(const uint64_t* __restrict__ keys, const uint32_t* __restrict__ vals,
+                             const int64_t* __restrict__ off, int64_t m, int rbits, int64_t nb,
+                             uint64_t* __restrict__ pkey, uint32_t* __restrict__ pval) {
+  const uint64_t rmask = (1ull << rbits) - 1ull;
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < m;
+       k += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t cnt = off[k + 1] - off[k];
+    if (cnt == 0) continue;
+    const int64_t ra = (int64_t)(keys[k] & rmask);
+    const float ua = __uint_as_float(vals[k]);
+    const int64_t I = ra / kBlockRows;
+    for (int64_t q = 0; q < cnt; ++q) {
+      const int64_t rb = (int64_t)(keys[k + 1 + q] & rmask);  // rows ascend: ra < rb
+      const int64_t J = rb / kBlockRows;
+      pkey[off[k] + q] = (tri_tile(I, J, nb) << 14) | ((uint64_t)(ra % kBlockRows) << 7) |
+                         (uint64_t)(rb % kBlockRows);
+      pval[off[k] + q] = (uint32_t)tail_fixed(ua * __uint_as_float(vals[k + 1 + q]));
+    }
+  }
+}
+
+// off[t] = first record of tile t (records sorted by tile), t = 0 .. ntiles.
+__global__ void k_tile_starts(const uint64_t* __restrict__ pkey, int64_t m, int64_t ntiles,
+                              uint32_t* __restrict__ off) {
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k <= m;
+       k += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t prev = k == 0 ? -1 : (int64_t)(pkey[k - 1] >> 14);
+    const int64_t cur = k == m ? ntiles : (int64_t)(pkey[k] >> 14);
+    for (int64_t t = prev + 1; t <= cur; ++t) off[t] = (uint32_t)k;
+  }
+}
+
+cuapss_status build_explicit_pairs(Side& s, const PrepOptions& o, int64_t* rcount, Workspace& ws,
+                                   const std::string& t, cudaStream_t st) {
+  const int64_t n = s.n, nb = s.nb;
+  int64_t* rptr = nullptr;
+  ST_TRY(ws.get(t + "rptr", (size_t)n + 1, &rptr));
+  ST_TRY(exclusive_scan<int64_t>(rcount, rptr, n, rptr + n, ws, t + "rptr", st));
+  int64_t m = 0;
+  CU_TRY(cudaMemcpyAsync(&m, rptr + n, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+  CU_TRY(cudaStreamSynchronize(st));
+  const int64_t ntiles = nb * (nb + 1) / 2;
+  uint32_t* off = nullptr;
+  ST_TRY(ws.get(t + "ex_off", (size_t)ntiles + 1, &off));
+  s.ex_off = off;
+  if (m < 2) {
+    CU_TRY(cudaMemsetAsync(off, 0, sizeof(uint32_t) * (ntiles + 1), st));
+    return CUAPSS_OK;
+  }
+  if (m >= (int64_t)UINT32_MAX - 1) return CUAPSS_EINVAL;
+  const int rbits = std::max(1, bits_for((uint64_t)n));
+  const int fbits = std::max(1, bits_for((uint64_t)(s.d - o.rare_from)));
+  uint64_t* keys = nullptr;
+  uint32_t* vals = nullptr;
+  ST_TRY(ws.get(t + "rare:keys", (size_t)m, &keys));
+  ST_TRY(ws.get(t + "rare:vals", (size_t)m, &vals));
+  k_rare_keys<<<grid_for(n * 32, kThreads), kThreads, 0, st>>>(s.rp2, s.col2, s.val2, rptr, n,
+                                                               o.rare_from, rbits, keys, vals);
+  LAUNCH_CHECK();
+  ST_TRY(radix_sort_pairs(keys, vals, m, rbits + fbits, ws, t + "rare", st));
+  int64_t* poff = nullptr;
+  ST_TRY(ws.get(t + "rare:poff", (size_t)m + 1, &poff));
+  k_rare_pair_counts<<<grid_for(m, kThreads), kThreads, 0, st>>>(keys, m, rbits,
+                                                                 o.rare_max_count, poff);
+  LAUNCH_CHECK();
+  ST_TRY(exclusive_scan<int64_t>(poff, poff, m, poff + m, ws, t + "rare:pscan", st));
+  int64_t P = 0;
+  CU_TRY(cudaMemcpyAsync(&P, poff + m, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+  CU_TRY(cudaStreamSynchronize(st));
+  if (P >= (int64_t)UINT32_MAX - 1) return CUAPSS_EINVAL;
+  s.n_explicit = P;
+  if (P == 0) {
+    CU_TRY(cudaMemsetAsync(off, 0, sizeof(uint32_t) * (ntiles + 1), st));
+    return CUAPSS_OK;
+  }
+  uint64_t* pkey = nullptr;
+  uint32_t* pval = nullptr;
+  ST_TRY(ws.get(t + "ex_key", (size_t)P, &pkey));
+  ST_TRY(ws.get(t + "ex_val", (size_t)P, &pval));
+  k_rare_pairs<<<grid_for(m, kThreads), kThreads, 0, st>>>(keys, vals, poff, m, rbits, nb, pkey,
+                                                           pval);
+  LAUNCH_CHECK();
+  ST_TRY(radix_sort_pairs(pkey, pval, P, bits_for((uint64_t)ntiles) + 14, ws, t + "ex", st));
+  k_tile_starts<<<grid_for(P + 1, kThreads), kThreads, 0, st>>>(pkey, P, ntiles, off);
+  LAUNCH_CHECK();
+  s.ex_key = pkey;
+  s.ex_val = reinterpret_cast<int32_t*>(pval);
+  return CUAPSS_OK;
+}
+
 }  // namespace
 
 cuapss_status validate_csr(const int64_t* rp, const int32_t* col, const float* val, int64_t n,
@@ -809,6 +958,64 @@ cuapss_status feature_perm(const int32_t* counts, int64_t d, int64_t max_count, 
   return CUAPSS_OK;
 }
 
+// Rare-feature statistics for candidate thresholds C[k]: out[2k] = features
+// occurring in more than C[k] rows, out[2k + 1] = pairs of the tail features
+// (rank >= p) occurring in at most C[k] rows.
+constexpr int kRareCands = 4;
+__host__ __device__ constexpr int rare_cand(int k) { return 128 >> k; }  // 128, 64, 32, 16
+
+__global__ void k_rare_stats(const int32_t* __restrict__ counts, const int32_t* __restrict__ perm,
+                             int64_t d, int p, unsigned long long* __restrict__ out) {
+  unsigned long long above[kRareCands] = {}, pairs[kRareCands] = {};
+  for (int64_t f = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; f < d;
+       f += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t c = counts[f];
+    const bool tail = perm[f] >= p;
+#pragma unroll
+    for (int k = 0; k < kRareCands; ++k) {
+      above[k] += c > rare_cand(k) ? 1ull : 0ull;
+      if (tail && c >= 2 && c <= rare_cand(k)) pairs[k] += (unsigned long long)(c * (c - 1) / 2);
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < kRareCands; ++k) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      above[k] += __shfl_xor_sync(0xffffffffu, above[k], o);
+      pairs[k] += __shfl_xor_sync(0xffffffffu, pairs[k], o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+      atomicAdd(&out[2 * k], above[k]);
+      atomicAdd(&out[2 * k + 1], pairs[k]);
+    }
+  }
+}
+
+cuapss_status choose_rare_features(const int32_t* counts, const int32_t* perm, int64_t d, int p,
+                                   int64_t max_pairs, Workspace& ws, cudaStream_t st,
+                                   int64_t* rare_from, int* max_count) {
+  *rare_from = 0;
+  *max_count = 0;
+  unsigned long long* out = nullptr;
+  ST_TRY(ws.get("rare:stats", 2 * kRareCands, &out));
+  CU_TRY(cudaMemsetAsync(out, 0, sizeof(unsigned long long) * 2 * kRareCands, st));
+  k_rare_stats<<<grid_for(d, kThreads), kThreads, 0, st>>>(counts, perm, d, p, out);
+  LAUNCH_CHECK();
+  unsigned long long h[2 * kRareCands];
+  CU_TRY(cudaMemcpyAsync(h, out, sizeof(h), cudaMemcpyDeviceToHost, st));
+  CU_TRY(cudaStreamSynchronize(st));
+  for (int k = 0; k < kRareCands; ++k) {
+    if ((int64_t)h[2 * k + 1] <= max_pairs) {
+      // features of count <= C hold the ranks >= (features above C); the
+      // head keeps its p ranks in any case
+      *rare_from = std::max<int64_t>((int64_t)h[2 * k], p);
+      *max_count = rare_cand(k);
+      return CUAPSS_OK;
+    }
+  }
+  return CUAPSS_OK;
+}
+
 cuapss_status rank_count_prefix(const int32_t* counts, int64_t d, int remap, int64_t m,
                                 Workspace& ws, cudaStream_t st, std::vector<int64_t>* prefix) {
   m = std::max<int64_t>(0, std::min(m, d));
@@ -840,7 +1047,6 @@ cuapss_status build_side(Side& s, const PrepOptions& o, const int32_t* perm, Wor
   const int nb = s.nb;
   const int rbits = std::max(1, bits_for((uint64_t)n));
   const int fbits = std::max(1, bits_for((uint64_t)d));
-  const uint64_t fmask = (fbits >= 64) ? ~0ull : ((1ull << fbits) - 1);
   const uint64_t rmask = (1ull << rbits) - 1;
   const std::string t = tag + ":";
   // ---- row order: the caller's, or tail-balanced blocks ----
@@ -878,6 +1084,12 @@ cuapss_status build_side(Side& s, const PrepOptions& o, const int32_t* perm, Wor
   ST_TRY(ws.get(t + "col2", (size_t)std::max<int64_t>(nnz, 1), &s.col2));
   ST_TRY(ws.get(t + "val2", (size_t)std::max<int64_t>(nnz, 1), &s.val2));
   int64_t* tcount = nullptr;
+  int64_t* rcount = nullptr;
+  if (o.rare_from > 0) ST_TRY(ws.get(t + "rcount", (size_t)n + 1, &rcount));
+  s.ex_off = nullptr;
+  s.ex_key = nullptr;
+  s.ex_val = nullptr;
+  s.n_explicit = 0;
   ST_TRY(ws.get(t + "hlen", (size_t)n, &s.hlen));
   ST_TRY(ws.get(t + "nnzrow", (size_t)n, &s.nnz_row));
   ST_TRY(ws.get(t + "hnorm", (size_t)n, &s.hnorm));
@@ -901,8 +1113,10 @@ cuapss_status build_side(Side& s, const PrepOptions& o, const int32_t* perm, Wor
   }
   k_split_rows<<<grid_for(n * 32, kThreads), kThreads, 0, st>>>(
       s.rp0, s.col0, s.val0, perm, place, s.rp2, n, p, s.col2, s.val2, s.hlen, s.nnz_row,
-      s.hnorm, tcount, s.blk_maxnnz, s.head16, nkc, s.head32);
+      s.hnorm, tcount, s.blk_maxnnz, s.head16, nkc, s.head32,
+      o.rare_from > 0 ? o.rare_from : INT64_MAX, o.rare_from > 0 ? rcount : nullptr);
   LAUNCH_CHECK();
+  if (o.rare_from > 0) ST_TRY(build_explicit_pairs(s, o, rcount, ws, t, st));
   ST_TRY(ws.get(t + "tptr", (size_t)n + 1, &s.tptr));
   ST_TRY(exclusive_scan<int64_t>(tcount, s.tptr, n, s.tptr + n, ws, t + "tptr", st));
   // ---- tail: segment pointers (blocks, J segments), host copies ----

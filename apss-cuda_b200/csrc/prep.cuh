@@ -16,6 +16,10 @@ struct PrepOptions {
   int want_head16 = 0;  // build the BF16 head block
   int want_csc = 0;     // build the global inverted lists (cptr/csc)
   int balance_rows = 0; // deal rows into blocks by tail non-zeros (rowperm); else caller order
+  // Self-joins: features of rank >= rare_from (each occurring in at most
+  // rare_max_count rows) are paired explicitly instead of probed; 0: off.
+  int64_t rare_from = 0;
+  int rare_max_count = 0;
 };
 
 // Validates a device CSR. counts (device, d entries, may be null) are
@@ -33,6 +37,14 @@ cuapss_status feature_perm(const int32_t* counts, int64_t d, int64_t max_count, 
 // (*prefix)[k] = postings of the k most frequent features, k = 0 .. min(m, d).
 cuapss_status rank_count_prefix(const int32_t* counts, int64_t d, int remap, int64_t m,
                                 Workspace& ws, cudaStream_t st, std::vector<int64_t>* prefix);
+
+// Rare features of a self-join (explicit pairs instead of probes): the
+// largest threshold C in {128, 64, 32, 16} whose tail features occurring in
+// at most C rows give at most max_pairs pairs; *rare_from = the first rank
+// of those features (>= p), *max_count = C; both 0 when none qualifies.
+cuapss_status choose_rare_features(const int32_t* counts, const int32_t* perm, int64_t d, int p,
+                                   int64_t max_pairs, Workspace& ws, cudaStream_t st,
+                                   int64_t* rare_from, int* max_count);
 
 // Builds every array of `s` (s.rp0/col0/val0/n/d/nnz must be set).
 cuapss_status build_side(Side& s, const PrepOptions& o, const int32_t* perm, Workspace& ws,

@@ -8,8 +8,9 @@
 //   rp2       int64[n+1]      copy of the caller's rowptr
 //   col2/val2 int32/f32[nnz]  the tail entries of each row (features of rank
 //                             >= p, remapped to their frequency rank), as a
-//                             suffix of the row's range of length
-//                             nnz - hlen[r]; the head prefix is not written
+//                             suffix of the row's range (tptr counts them);
+//                             for a self-join the rare features' entries as
+//                             its prefix; the head entries are not written
 //   head32    f32[nb][p][128] dense head block, k-major inside a row block so
 //                             that a 32-feature slice of a block is one
 //                             contiguous 16 KB run (one bulk TMA copy)
@@ -76,6 +77,13 @@ struct Side {
   int64_t max_block_tail = 0;
   std::vector<int64_t> h_bptr;    // host copy of bptr (unit scheduling)
   int64_t tail_products = 0;      // sum over tail lists of L(L-1)/2
+  // explicit pairs of the rare features (self-joins): records sorted by
+  // triangular tile index, {tile << 14 | row in I block << 7 | column in J
+  // block} with the fixed-point product; ex_off[t] = first record of tile t
+  uint32_t* ex_off = nullptr;
+  uint64_t* ex_key = nullptr;
+  int32_t* ex_val = nullptr;
+  int64_t n_explicit = 0;
   double nrm_max = 1.0;           // largest row norm (FP64)
 };
 

@@ -137,6 +137,26 @@ __device__ __forceinline__ int acc_cell(int r, int c, int ld) {
   return SWZ ? r * 32 + ((((c >> 2) ^ (r & 7)) << 2) | (c & 3)) : r * ld + c;
 }
 
+// Triangular index of tile (I, J), J >= I, among nb row blocks.
+__host__ __device__ __forceinline__ int64_t tile_index(int64_t I, int64_t J, int64_t nb) {
+  return I * nb - I * (I - 1) / 2 + (J - I);
+}
+
+// Adds the explicit rare-feature records [lo, hi) of a tile whose column
+// lies in [cofs, cofs + ncols) into acc at acc_cell<SWZ>(row, column - cofs);
+// thread tid of nthreads.
+template <bool SWZ>
+__device__ __forceinline__ void tail_explicit(const TileArgs& A, uint32_t lo, uint32_t hi,
+                                              int* acc, int ld, int cofs, int ncols, int tid,
+                                              int nthreads) {
+  for (uint32_t k = lo + (uint32_t)tid; k < hi; k += (uint32_t)nthreads) {
+    const uint64_t key = __ldg(&A.ex_key[k]);
+    const int c = (int)(key & 127u) - cofs;
+    if (c >= 0 && c < ncols)
+      atomicAdd(acc + acc_cell<SWZ>((int)((key >> 7) & 127u), c, ld), __ldg(&A.ex_val[k]));
+  }
+}
+
 // Products of one J posting (feature f, column c, value v) with the staged
 // I postings of feature f.
 template <bool SWZ>

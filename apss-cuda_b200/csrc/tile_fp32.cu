@@ -125,6 +125,11 @@ __global__ void __launch_bounds__(kThreads, 1) k_tiles_fp32(const TileArgs A) {
               __syncthreads();  // staging rewritten by the next chunk
             }
           }
+          if (A.ex_off) {  // explicit pairs of the rare features
+            const int64_t te = tile_index(I, J, A.nbI);
+            tail_explicit<false>(A, A.ex_off[te], A.ex_off[te + 1], acc, kAccLd, 0, kBlockRows,
+                                 tid, kThreads);
+          }
         }
         // ---- head: FP32 FMA chain over the p head features
         float h[8][8];

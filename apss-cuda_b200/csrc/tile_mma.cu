@@ -375,10 +375,22 @@ __global__ void __launch_bounds__(kThreads, 1) k_tiles_mma(const TileArgs A, con
       for (int m = 0; m <= kJSegs; ++m) hc[m] = (uint32_t)A.hptrJ[kJSegs * U.y + m];
       uint2 nxt[kBatch];
       load_batch<kBatch>(A, hc[0], hc[1], ttid, kTT, nxt);
+      // explicit rare-feature records of the current and the next tile
+      uint32_t ec0 = 0, ec1 = 0, en0 = 0, en1 = 0;
+      if (A.ex_off) {
+        const int64_t t0 = tile_index(I, U.y, A.nbI);
+        ec0 = A.ex_off[t0];
+        ec1 = A.ex_off[t0 + 1];
+      }
       for (int J = U.y; J < U.z; ++J) {
         if (J + 1 < U.z) {
 #pragma unroll
           for (int m = 0; m <= kJSegs; ++m) hn[m] = (uint32_t)A.hptrJ[kJSegs * (J + 1) + m];
+          if (A.ex_off) {
+            const int64_t t1 = tile_index(I, J + 1, A.nbI);
+            en0 = A.ex_off[t1];
+            en1 = A.ex_off[t1 + 1];
+          }
         }
 #pragma unroll
         for (int q = 0; q < kSlabs; ++q, ++g) {
@@ -408,11 +420,15 @@ __global__ void __launch_bounds__(kThreads, 1) k_tiles_mma(const TileArgs A, con
               named_bar(kTailBar, kTT);  // staging rewritten by the next chunk
             }
           }
+          if (live && ec1 > ec0)
+            tail_explicit<true>(A, ec0, ec1, acc, kSlabCols, cofs, kSlabCols, ttid, kTT);
           __syncwarp();
           if (live && lane == 0) mbar_arrive(&S.afull[k]);
         }
 #pragma unroll
         for (int m = 0; m <= kJSegs; ++m) hc[m] = hn[m];
+        ec0 = en0;
+        ec1 = en1;
       }
     }
   } else {

@@ -37,6 +37,11 @@ struct TileArgs {
   const float* hnormJ;
   const int64_t* hptrJ;     // postings of each kJSegRows-row segment of J
   const uint2* bilJ_rec;    // packed postings {feature << 8 | row, value bits}
+  // explicit pairs of rare features (self-joins; null: none): records of
+  // tile (I, J) at [ex_off[t], ex_off[t + 1]), t = tri_tile(I, J, nbI)
+  const uint32_t* ex_off;
+  const uint64_t* ex_key;
+  const int32_t* ex_val;
   int p;
   int self;
   float t;
