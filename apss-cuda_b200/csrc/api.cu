@@ -181,8 +181,9 @@ cuapss_status join_device(cuapss_ctx* ctx, const DevCsr& a, const DevCsr* b, flo
   po.want_head16 = mixed ? 1 : 0;
   // Tail features that occur in at most a few rows are paired explicitly
   // (self-joins on one shard): probing their postings in every tile is
-  // almost all misses.
-  if (self && nshards == 1)
+  // almost all misses. They are the highest ranks only under the frequency
+  // remap.
+  if (self && nshards == 1 && ctx->opts.remap)
     ST_TRY(choose_rare_features(counts, perm, d, p, kMaxExplicitPairs, ws, st, &po.rare_from,
                                 &po.rare_max_count));
   Side SA, SB;

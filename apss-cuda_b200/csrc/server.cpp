@@ -30,12 +30,19 @@
 // output). A batch is admitted while the estimates of all batches in flight
 // stay within hbm_budget; a lone batch is always admitted.
 //
+// Streams. Each lane's context runs on a stream of the device's highest
+// priority; appends run on one separate context whose stream has the lowest
+// priority, so the block scheduler starts pending query CTAs ahead of an
+// append's or a merge's (appends are serialised by the index anyway).
+//
 // Appends are taken in submission order by one lane at a time, when they
 // are the oldest queued item; queries queued behind an append wait until
 // some lane has taken it. A request is matched against the index rows that
 // existed when the first of its batches started (for a sliced request, the
 // fewest rows any of its slices saw; pairs with rows appended later are
 // dropped), reported in cuapss_request_info.index_rows.
+#include <cuda_runtime.h>
+
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
@@ -100,6 +107,8 @@ struct cuapss_server {
   cuapss_server_opts opts{};
   int head_width = 0;
   std::vector<cuapss_ctx*> lanes;
+  cuapss_ctx* append_ctx = nullptr;      // appends and merges, low-priority stream
+  std::vector<cudaStream_t> streams;     // created here, destroyed after the contexts
   std::vector<std::thread> threads;
   std::mutex mu;
   std::condition_variable cv_work, cv_done;
@@ -348,7 +357,7 @@ void lane_loop(cuapss_server* s, int lane) {
         s->cv_work.wait(lk);
       }
     }
-    if (app) run_append(s, ctx, app);
+    if (app) run_append(s, s->append_ctx, app);
     else run_batch(s, ctx, batch, bid, est);
     s->cv_done.notify_all();
     s->cv_work.notify_all();
@@ -434,17 +443,36 @@ cuapss_status cuapss_server_create(cuapss_server** out, cuapss_index* idx, int d
   cuapss_status st = cuapss_index_info(idx, nullptr, nullptr, &p, nullptr);
   if (st != CUAPSS_OK) return st;
   s->head_width = p;
-  for (int l = 0; l < opts.lanes; ++l) {
+  auto undo = [&s]() {
+    for (auto* x : s->lanes) cuapss_destroy(x);
+    if (s->append_ctx) cuapss_destroy(s->append_ctx);
+    for (auto q : s->streams) cudaStreamDestroy(q);
+  };
+  int least = 0, greatest = 0;
+  if (cudaSetDevice(device) != cudaSuccess ||
+      cudaDeviceGetStreamPriorityRange(&least, &greatest) != cudaSuccess)
+    return CUAPSS_ECUDA;
+  for (int l = 0; l <= opts.lanes; ++l) {  // the lanes, then the append context
+    const bool append = l == opts.lanes;
+    cudaStream_t q = nullptr;
+    if (cudaStreamCreateWithPriority(&q, cudaStreamNonBlocking, append ? least : greatest) !=
+        cudaSuccess) {
+      undo();
+      return CUAPSS_ECUDA;
+    }
+    s->streams.push_back(q);
     cuapss_opts co;
     cuapss_default_opts(&co);
     co.device = device;
+    co.stream = q;
     cuapss_ctx* c = nullptr;
     st = cuapss_create(&c, &co);
     if (st != CUAPSS_OK) {
-      for (auto* x : s->lanes) cuapss_destroy(x);
+      undo();
       return st;
     }
-    s->lanes.push_back(c);
+    if (append) s->append_ctx = c;
+    else s->lanes.push_back(c);
   }
   for (int l = 0; l < opts.lanes; ++l) s->threads.emplace_back(lane_loop, s.get(), l);
   *out = s.release();
@@ -524,6 +552,8 @@ cuapss_status cuapss_server_destroy(cuapss_server* s) {
   s->cv_work.notify_all();
   for (auto& th : s->threads) th.join();
   for (auto* c : s->lanes) cuapss_destroy(c);
+  if (s->append_ctx) cuapss_destroy(s->append_ctx);
+  for (auto q : s->streams) cudaStreamDestroy(q);
   delete s;
   return CUAPSS_OK;
 }
