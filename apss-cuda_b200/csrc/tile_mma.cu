@@ -72,7 +72,7 @@ static_assert(kEpiCols == 16 || kEpiCols == 32, "tensor-memory loads of 16 or 32
 constexpr uint32_t kTmemCols = 256;
 constexpr int kTailBar = 1;
 constexpr int kEpiBar = 2;
-constexpr int kBatch = 3;                     // J postings per thread per load batch
+constexpr int kBatch = 2;                     // J postings per thread per load batch
 constexpr int kUnitRing = 8;                  // unit ids published ahead by the producer
 constexpr int kUnitReaders = 1 + kTW + kEW;   // MMA thread + tail warps + epilogue warps
 static_assert(kSlabCols == 32, "slab accumulator rows are 32 ints (8 swizzled groups)");
@@ -193,6 +193,20 @@ __device__ __forceinline__ void probe_batch(const TailStage& S, const uint2 (&re
     if (rec[q].x == 0xffffffffu) break;  // the rest of the batch is past the range
     tail_probe<true>(S, rec[q].x >> 8, (int)(rec[q].x & 0xffu) - cofs, __uint_as_float(rec[q].y),
                      acc, kSlabCols);
+  }
+}
+
+// Thread tid's explicit rare-feature record of a tile whose records are
+// [lo, hi): {row in I block << 7 | column in J block} and its fixed-point
+// product, or kNoRecord.
+constexpr uint32_t kNoRecord = 0xffffffffu;
+__device__ __forceinline__ void load_record(const TileArgs& A, uint32_t lo, uint32_t hi, int tid,
+                                            uint32_t& rc, int& rv) {
+  rc = kNoRecord;
+  rv = 0;
+  if (lo + (uint32_t)tid < hi) {
+    rc = (uint32_t)(__ldg(&A.ex_key[lo + tid]) & 0x3fffu);
+    rv = __ldg(&A.ex_val[lo + tid]);
   }
 }
 
@@ -375,12 +389,17 @@ __global__ void __launch_bounds__(kThreads, 1) k_tiles_mma(const TileArgs A, con
       for (int m = 0; m <= kJSegs; ++m) hc[m] = (uint32_t)A.hptrJ[kJSegs * U.y + m];
       uint2 nxt[kBatch];
       load_batch<kBatch>(A, hc[0], hc[1], ttid, kTT, nxt);
-      // explicit rare-feature records of the current and the next tile
+      // explicit rare-feature records: the bounds of the current and the next
+      // tile, and this thread's record of each (loaded two slabs ahead; a
+      // tile's records beyond the first kTT are loaded where they are used)
       uint32_t ec0 = 0, ec1 = 0, en0 = 0, en1 = 0;
+      uint32_t rc = kNoRecord, rn = kNoRecord;
+      int rv = 0, rnv = 0;
       if (A.ex_off) {
         const int64_t t0 = tile_index(I, U.y, A.nbI);
         ec0 = A.ex_off[t0];
         ec1 = A.ex_off[t0 + 1];
+        load_record(A, ec0, ec1, ttid, rc, rv);
       }
       for (int J = U.y; J < U.z; ++J) {
         if (J + 1 < U.z) {
@@ -402,6 +421,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_tiles_mma(const TileArgs A, con
           // the next slab of this unit: its first batch, in flight from here
           if (q + 1 < kSlabs) load_batch<kBatch>(A, hc[q + 1], hc[q + 2], ttid, kTT, nxt);
           else if (J + 1 < U.z) load_batch<kBatch>(A, hn[0], hn[1], ttid, kTT, nxt);
+          if (q == kSlabs - 2 && A.ex_off && J + 1 < U.z) load_record(A, en0, en1, ttid, rn, rnv);
           live = warp_wait(A, &S.aempty[k], (use & 1u) ^ 1u, abort, live);
           int* acc = S.acc + k * kSlabInts;
           const int cofs = q * kSlabCols;
@@ -420,8 +440,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_tiles_mma(const TileArgs A, con
               named_bar(kTailBar, kTT);  // staging rewritten by the next chunk
             }
           }
-          if (live && ec1 > ec0)
-            tail_explicit<true>(A, ec0, ec1, acc, kSlabCols, cofs, kSlabCols, ttid, kTT);
+          if (live && rc != kNoRecord && (int)((rc & 127u) >> 5) == q)
+            atomicAdd(acc + acc_cell<true>((int)(rc >> 7), (int)(rc & 31u), kSlabCols), rv);
+          if (live && ec1 - ec0 > (uint32_t)kTT)
+            tail_explicit<true>(A, ec0 + kTT, ec1, acc, kSlabCols, cofs, kSlabCols, ttid, kTT);
           __syncwarp();
           if (live && lane == 0) mbar_arrive(&S.afull[k]);
         }
@@ -429,6 +451,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_tiles_mma(const TileArgs A, con
         for (int m = 0; m <= kJSegs; ++m) hc[m] = hn[m];
         ec0 = en0;
         ec1 = en1;
+        rc = rn;
+        rv = rnv;
       }
     }
   } else {
