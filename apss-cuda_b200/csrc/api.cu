@@ -41,45 +41,126 @@ const char* last_error_message() { return g_last_error; }
 
 // Per-tile cost model of the mixed-precision tile kernel, whose tensor-core
 // side and sparse-tail side mostly overlap, so the slower one sets the pace:
-//   head  kHeadChunkNs per 64 head features (operand stream and MMAs of a
+//   head  head_chunk_ns per 64 head features (operand stream and MMAs of a
 //         128 x 128 tile),
-//   tail  kTailPostingNs per tail posting of the J block (one probe of the
-//         staged I postings); a block holds 128 x (tail non-zeros per row),
-//   cost  max(head, tail) + kOverlapLoss x min(head, tail).
-// Fitted to tile-kernel times on the n = d = 1M workload's shape at 200,000
-// rows for p = 768 .. 2048. The head width p minimises the cost over
-// multiples of 64; the tail non-zeros at each p come from the posting counts
-// in frequency order.
-// Explicit rare-feature pairs of one self-join (12 bytes each, twice for the
-// sort): at most 400M.
-constexpr int64_t kMaxExplicitPairs = 400000000;
+//   tail  tail_posting_ns per probed tail posting of the J block (one probe
+//         of the staged I postings); a block holds 128 x (probed tail
+//         non-zeros per row),
+//   cost  max(head, tail) + overlap_loss x min(head, tail).
+// Fitted to tile-kernel times on the n = d = 1M workload's shape: with
+// every tail feature probed at 200,000 rows for p = 768 .. 2048, and with
+// the rare features paired explicitly at 200,000 and 1,000,000 rows for
+// p = 640 .. 1152 and C = 128 .. 2048 (their postings leave the probed
+// tail; the probes left are the costlier hits of the frequent tail
+// features). The head width p minimises the cost over multiples of 64; the
+// tail non-zeros at each p come from the posting counts in frequency order.
+// Explicit rare-feature pairs of one self-join: 8-byte records, offsets of
+// 32 bits; the records take at most 40% of the free device memory.
+constexpr int64_t kMaxExplicitPairs = 4000000000;
+constexpr double kExplicitPairBytes = 8.0, kExplicitMemShare = 0.4;
+// Cost of one explicit pair in SM-nanoseconds, against the per-tile cost
+// below (SM-nanoseconds of one 128 x 128 tile): its addition in the tile
+// kernel (about 4) and its share of the build's count and placement passes
+// (about 3.5), measured on the n = d = 1M workload's shape.
+constexpr double kExplicitPairSmNs = 7.5;
 
-constexpr double kHeadChunkNs = 388.0;
-constexpr double kTailPostingNs = 1.6;
-constexpr double kOverlapLoss = 0.06;
+struct TileCostModel {
+  double head_chunk_ns, tail_posting_ns, overlap_loss;
+};
+constexpr TileCostModel kProbedTail{388.0, 1.6, 0.06};
+constexpr TileCostModel kRarePaired{340.0, 1.84, 0.3};
 constexpr int kMaxModelHead = 8192;
 
+namespace {
+
+// Tail postings still probed at head width p (ranks >= p), without the
+// paired rare features (ranks >= rare_rank) when rare_postings > 0.
+int64_t probed_postings(int64_t p, int64_t nnz, const std::vector<int64_t>& prefix,
+                        int64_t rare_rank, int64_t rare_postings) {
+  const int64_t top = (int64_t)prefix.size() - 1;
+  int64_t probed = nnz - prefix[(size_t)std::min(p, top)];
+  if (rare_postings > 0) probed = p < rare_rank ? std::max<int64_t>(0, probed - rare_postings) : 0;
+  return probed;
+}
+
+// Modelled SM-nanoseconds of one tile at head width p. The FP32 head runs
+// on CUDA cores beside nothing: only its tail side depends on the split.
+double tile_ns(int precision, int64_t p, int64_t n, int64_t probed, bool paired) {
+  const TileCostModel& m = paired ? kRarePaired : kProbedTail;
+  const double tail = m.tail_posting_ns * kBlockRows * ((double)probed / (double)n);
+  if (precision != CUAPSS_PREC_MIXED) return tail;
+  const double head = m.head_chunk_ns * (double)(p / 64);
+  return std::max(head, tail) + m.overlap_loss * std::min(head, tail);
+}
+
+// The model's head width and its tile cost.
+int best_head_width(int64_t n, int64_t nnz, const std::vector<int64_t>& prefix, int64_t rare_rank,
+                    int64_t rare_postings, double* cost) {
+  double best = 1e300;
+  int best_p = 64;
+  const int64_t top = (int64_t)prefix.size() - 1;  // ranks with known counts
+  for (int64_t p = 64; p <= std::min<int64_t>(top, kMaxModelHead); p += 64) {
+    const int64_t probed = probed_postings(p, nnz, prefix, rare_rank, rare_postings);
+    const double c = tile_ns(CUAPSS_PREC_MIXED, p, n, probed, rare_postings > 0);
+    if (c < best - 1e-9) {
+      best = c;
+      best_p = (int)p;
+    }
+  }
+  *cost = best;
+  return best_p;
+}
+
+}  // namespace
+
 int choose_head_width(int precision, int64_t n, int64_t d, int64_t nnz,
-                      const std::vector<int64_t>& prefix) {
+                      const std::vector<int64_t>& prefix, int64_t rare_rank,
+                      int64_t rare_postings) {
   const int64_t cap = ((d + 31) / 32) * 32;
   // the FP32 head runs on CUDA cores and pays per feature per pair: its
   // measured optimum on the lognormal/Zipf workloads is a narrow head
   if (precision != CUAPSS_PREC_MIXED) return (int)std::min<int64_t>(64, cap);
   if (n <= 0 || prefix.size() < 2) return (int)std::min<int64_t>(1024, ((d + 63) / 64) * 64);
-  double best = 1e300;
-  int best_p = 64;
-  const int64_t top = (int64_t)prefix.size() - 1;  // ranks with known counts
-  for (int64_t p = 64; p <= std::min<int64_t>(top, kMaxModelHead); p += 64) {
-    const double tail_per_row = (double)(nnz - prefix[(size_t)p]) / (double)n;
-    const double head = kHeadChunkNs * (double)(p / 64);
-    const double tail = kTailPostingNs * kBlockRows * tail_per_row;
-    const double cost = std::max(head, tail) + kOverlapLoss * std::min(head, tail);
-    if (cost < best - 1e-9) {
+  double cost = 0.0;
+  return best_head_width(n, nnz, prefix, rare_rank, rare_postings, &cost);
+}
+
+TilePlan plan_tiles(int precision, int64_t n, int64_t d, int64_t nnz,
+                    const std::vector<int64_t>& prefix,
+                    const std::vector<RareCandidate>& cands, int64_t max_pairs, int fixed_p,
+                    bool forced) {
+  TilePlan plan;
+  plan.p = fixed_p > 0 ? fixed_p : choose_head_width(precision, n, d, nnz, prefix);
+  if (cands.empty() || n <= 0 || prefix.size() < 2) return plan;
+  const double nbk = std::ceil((double)n / kBlockRows);
+  const double tiles = nbk * (nbk + 1.0) / 2.0;
+  auto cost_at = [&](const RareCandidate* c, int* p_out) {
+    const int64_t rank = c ? c->rank : 0, posts = c ? c->postings : 0;
+    double per_tile = 0.0;
+    int p = fixed_p;
+    if (precision == CUAPSS_PREC_MIXED && fixed_p <= 0) {
+      p = best_head_width(n, nnz, prefix, rank, posts, &per_tile);
+    } else {
+      if (p <= 0) p = plan.p;
+      per_tile = tile_ns(precision, p, n, probed_postings(p, nnz, prefix, rank, posts), c != nullptr);
+    }
+    *p_out = p;
+    return tiles * per_tile + (c ? (double)c->pairs * kExplicitPairSmNs : 0.0);
+  };
+  int p0 = plan.p;
+  double best = cost_at(nullptr, &p0);
+  plan.p = p0;
+  for (const RareCandidate& c : cands) {
+    if (c.pairs > max_pairs || c.pairs >= (int64_t)UINT32_MAX - 1) continue;
+    int pc = 0;
+    const double cost = cost_at(&c, &pc);
+    if (cost < best || forced) {
       best = cost;
-      best_p = (int)p;
+      plan.p = pc;
+      plan.rare = c;
     }
   }
-  return best_p;
+  return plan;
 }
 
 cuapss_status stage_csr(cuapss_ctx* ctx, const cuapss_csr* x, const std::string& tag,
@@ -156,14 +237,38 @@ cuapss_status join_device(cuapss_ctx* ctx, const DevCsr& a, const DevCsr* b, flo
     nrm_b = nrm_a;
   ST_TRY(feature_perm(counts, d, a.n + (self ? 0 : bb.n), ctx->opts.remap, perm, ws, st));
   const int precision = ctx->opts.precision;
-  int p = ctx->opts.head_width;
-  if (p <= 0) {
-    std::vector<int64_t> prefix;
-    if (precision == CUAPSS_PREC_MIXED)
-      ST_TRY(rank_count_prefix(counts, d, ctx->opts.remap, kMaxModelHead, ws, st, &prefix));
-    const int64_t n_all = a.n + (self ? 0 : bb.n), nnz_all = a.nnz + (self ? 0 : bb.nnz);
-    p = choose_head_width(precision, n_all, d, nnz_all, prefix);
+  // Tail features that occur in at most a few rows are paired explicitly
+  // (self-joins on one shard): probing their postings in every tile is
+  // almost all misses. They are the highest ranks only under the frequency
+  // remap. The threshold and the head width are chosen together: the head
+  // is sized against the tail that is still probed, each threshold's pairs
+  // cost their build and their additions.
+  std::vector<RareCandidate> rare;
+  const int forced_rare = ctx->opts.rare_max_count;
+  if (self && nshards == 1 && ctx->opts.remap && forced_rare >= 0) {
+    ST_TRY(rare_feature_candidates(counts, d, ws, st, &rare));
+    if (forced_rare > 0) {
+      std::vector<RareCandidate> keep;
+      for (const RareCandidate& c : rare)
+        if (c.max_count == forced_rare) keep.push_back(c);
+      rare.swap(keep);
+    }
   }
+  const int64_t n_all = a.n + (self ? 0 : bb.n), nnz_all = a.nnz + (self ? 0 : bb.nnz);
+  std::vector<int64_t> prefix;
+  if ((precision == CUAPSS_PREC_MIXED && ctx->opts.head_width <= 0) || !rare.empty())
+    ST_TRY(rank_count_prefix(counts, d, ctx->opts.remap, kMaxModelHead, ws, st, &prefix));
+  int64_t max_pairs = 0;
+  if (!rare.empty()) {
+    size_t free_b = 0, total_b = 0;
+    CU_TRY(cudaMemGetInfo(&free_b, &total_b));
+    max_pairs = std::min<int64_t>(
+        kMaxExplicitPairs, (int64_t)((double)free_b * kExplicitMemShare / kExplicitPairBytes));
+  }
+  if (forced_rare > 0 && !rare.empty() && rare[0].pairs > max_pairs) return CUAPSS_ENOMEM;
+  const TilePlan plan = plan_tiles(precision, n_all, d, nnz_all, prefix, rare, max_pairs,
+                                   ctx->opts.head_width, forced_rare > 0);
+  int p = plan.p;
   const bool mixed = precision == CUAPSS_PREC_MIXED;
   const int pq = mixed ? 64 : 32;  // head width granularity of the tile kernels
   p = (int)std::min<int64_t>(((int64_t)p + pq - 1) / pq * pq, ((d + pq - 1) / pq) * pq);
@@ -179,13 +284,11 @@ cuapss_status join_device(cuapss_ctx* ctx, const DevCsr& a, const DevCsr* b, flo
   po.balance_rows = nshards == 1 ? 1 : 0;
   po.want_head32 = mixed ? 0 : 1;
   po.want_head16 = mixed ? 1 : 0;
-  // Tail features that occur in at most a few rows are paired explicitly
-  // (self-joins on one shard): probing their postings in every tile is
-  // almost all misses. They are the highest ranks only under the frequency
-  // remap.
-  if (self && nshards == 1 && ctx->opts.remap)
-    ST_TRY(choose_rare_features(counts, perm, d, p, kMaxExplicitPairs, ws, st, &po.rare_from,
-                                &po.rare_max_count));
+  if (plan.rare.max_count > 0) {
+    // the head keeps its p ranks in any case
+    po.rare_from = std::max<int64_t>(plan.rare.rank, p);
+    po.rare_max_count = plan.rare.max_count;
+  }
   Side SA, SB;
   SA.rp0 = a.rp;
   SA.col0 = a.col;
@@ -231,8 +334,7 @@ cuapss_status join_device(cuapss_ctx* ctx, const DevCsr& a, const DevCsr* b, flo
   ta.bilJ_rec = SJ->bil_rec;
   if (self && SA.n_explicit > 0) {
     ta.ex_off = SA.ex_off;
-    ta.ex_key = SA.ex_key;
-    ta.ex_val = SA.ex_val;
+    ta.ex_rec = SA.ex_rec;
   }
   ta.p = SA.p;
   ta.self = self ? 1 : 0;
@@ -399,6 +501,8 @@ cuapss_status join_device(cuapss_ctx* ctx, const DevCsr& a, const DevCsr* b, flo
     stats->ms_finalize = elapsed(ctx->ev[2], ctx->ev[3]);
     stats->ms_total = elapsed(ctx->ev[0], ctx->ev[3]);
     stats->launches = g_launches.load() - launches0;
+    stats->explicit_pairs = SA.n_explicit;
+    stats->rare_max_count = po.rare_max_count;
   }
   return result;
 }
@@ -420,6 +524,7 @@ void cuapss_default_opts(cuapss_opts* o) {
   o->validate = 1;
   o->norm_tol = 1e-4f;
   o->verbose = 0;
+  o->rare_max_count = 0;
 }
 
 const char* cuapss_status_string(cuapss_status s) {
@@ -445,6 +550,10 @@ cuapss_status cuapss_create(cuapss_ctx** out, const cuapss_opts* opts) {
   else cuapss_default_opts(&o);
   if (o.precision != CUAPSS_PREC_FP32 && o.precision != CUAPSS_PREC_MIXED) return CUAPSS_EINVAL;
   if (o.head_width < 0 || !(o.norm_tol >= 0.0f)) return CUAPSS_EINVAL;
+  if (o.rare_max_count < -1 || o.rare_max_count > kMaxRareCount ||
+      (o.rare_max_count > 0 && (o.rare_max_count < 16 ||
+                                (o.rare_max_count & (o.rare_max_count - 1)) != 0)))
+    return CUAPSS_EINVAL;
   int ndev = 0;
   CU_TRY(cudaGetDeviceCount(&ndev));
   if (o.device < 0 || o.device >= ndev) return CUAPSS_EINVAL;

@@ -9,6 +9,7 @@
 
 #include "common.cuh"
 #include "cuapss.h"
+#include "prep.cuh"
 #include "side.cuh"
 
 struct cuapss_ctx {
@@ -48,8 +49,25 @@ cuapss_status join_device(cuapss_ctx* ctx, const DevCsr& a, const DevCsr* b, flo
 
 // Head width used when the options leave it to the library: n rows, nnz
 // non-zeros over d features; prefix[k] = postings of the k most frequent
-// features (rank_count_prefix; may be empty for FP32).
+// features (rank_count_prefix; may be empty for FP32). Self-joins whose rare
+// features are paired explicitly pass the first rank of those features and
+// their postings (0: every tail feature is probed).
 int choose_head_width(int precision, int64_t n, int64_t d, int64_t nnz,
-                      const std::vector<int64_t>& prefix);
+                      const std::vector<int64_t>& prefix, int64_t rare_rank = 0,
+                      int64_t rare_postings = 0);
+
+// Head width and rare-feature threshold of a self-join, chosen together by
+// the tile cost model: the threshold (of cands, at most max_pairs pairs, or
+// none) and p that minimise the modelled tile time plus the explicit pairs'
+// cost. fixed_p > 0: that head width, the threshold alone is chosen.
+// forced: the (single) candidate is taken whatever its modelled cost.
+struct TilePlan {
+  int p = 0;
+  RareCandidate rare;  // max_count 0: no explicit pairs
+};
+TilePlan plan_tiles(int precision, int64_t n, int64_t d, int64_t nnz,
+                    const std::vector<int64_t>& prefix,
+                    const std::vector<RareCandidate>& cands, int64_t max_pairs, int fixed_p,
+                    bool forced = false);
 
 }  // namespace cuapss

@@ -744,75 +744,217 @@ cuapss_status launch_seg_sorts(const int32_t* idsB, const int (&fB)[kSegClasses 
 // A feature that occurs in at most a few rows is a waste to probe: its J
 // postings meet the I blocks' staged lists of almost every tile for nothing.
 // Its pairs are enumerated instead: the rare entries are sorted by (feature,
-// row), every pair of postings of one feature gives a record {triangular
-// tile index << 14 | row in I block << 7 | column in J block} with the
-// fixed-point product, and the records are sorted by tile, so that a tile
-// adds its few records to its tail accumulator directly.
+// row); every pair of postings of one feature gives a record {fixed-point
+// product << 32 | row in I block << 7 | column in J block}, grouped by
+// triangular tile index, so that a tile adds its records to its tail
+// accumulator directly. The grouping is a counting sort done per tile row:
+// one CTA per I block walks the pairs whose first row lies in the block,
+// counts them per J block in shared memory, and after a scan of the counts
+// over all tiles places them from shared-memory cursors, so that each CTA
+// writes one contiguous range. The order of records within a tile is not
+// fixed: the accumulator's integer additions do not depend on it.
 
 // One warp per row: its rare entries (the row's prefix) as sort keys
-// {rare feature << rbits | row} with the value bits.
+// {rare feature << rbits | row}, their row-major index as the payload, and
+// their value bits in row-major order.
 __global__ void k_rare_keys(const int64_t* __restrict__ rp2, const int32_t* __restrict__ col2,
                             const float* __restrict__ val2, const int64_t* __restrict__ rptr,
                             int64_t n, int64_t rare_from, int rbits, uint64_t* __restrict__ keys,
-                            uint32_t* __restrict__ vals) {
+                            uint32_t* __restrict__ idx, uint32_t* __restrict__ vrm) {
   const int lane = threadIdx.x & 31;
   const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
   for (int64_t r = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; r < n; r += warps) {
     const int64_t o = rptr[r], m = rptr[r + 1] - o, lo = rp2[r];
     for (int64_t k = lane; k < m; k += 32) {
       keys[o + k] = ((uint64_t)(col2[lo + k] - rare_from) << rbits) | (uint64_t)r;
-      vals[o + k] = __float_as_uint(val2[lo + k]);
+      idx[o + k] = (uint32_t)(o + k);
+      vrm[o + k] = __float_as_uint(val2[lo + k]);
     }
   }
 }
 
-// Pairs that posting k of the sorted rare list opens: the later postings of
-// its feature (a feature has at most max_run postings).
+// After the sort: vs[k] = value of sorted posting k, inv[row-major index] = k.
+__global__ void k_rare_gather(const uint32_t* __restrict__ idx, const uint32_t* __restrict__ vrm,
+                              int64_t m, uint32_t* __restrict__ vs, uint32_t* __restrict__ inv) {
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < m;
+       k += (int64_t)gridDim.x * blockDim.x) {
+    const uint32_t i = idx[k];
+    vs[k] = vrm[i];
+    inv[i] = (uint32_t)k;
+  }
+}
+
+// Pairs that sorted posting k opens: the later postings of its feature (a
+// feature has at most max_run postings; binary search for the end of its
+// run). The total is added to *total.
 __global__ void k_rare_pair_counts(const uint64_t* __restrict__ keys, int64_t m, int rbits,
-                                   int max_run, int64_t* __restrict__ cnt) {
+                                   int max_run, int32_t* __restrict__ cnt,
+                                   unsigned long long* __restrict__ total) {
+  unsigned long long sum = 0;
   for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < m;
        k += (int64_t)gridDim.x * blockDim.x) {
     const uint64_t f = keys[k] >> rbits;
-    int64_t e = k + 1;
-    while (e < m && e - k <= max_run && (keys[e] >> rbits) == f) ++e;
-    cnt[k] = e - k - 1;
+    int64_t lo = k + 1, hi = k + max_run < m ? k + max_run : m;  // run end in [lo, hi]
+    while (lo < hi) {
+      const int64_t mid = (lo + hi) >> 1;
+      if ((keys[mid] >> rbits) == f) lo = mid + 1;
+      else hi = mid;
+    }
+    cnt[k] = (int32_t)(lo - k - 1);
+    sum += (unsigned long long)(lo - k - 1);
   }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+  if ((threadIdx.x & 31) == 0 && sum) atomicAdd(total, sum);
 }
 
-__device__ __forceinline__ uint64_t tri_tile(int64_t I, int64_t J, int64_t nb) {
-  return (uint64_t)(I * nb - I * (I - 1) / 2 + (J - I));
-}
+constexpr int kRareTileChunk = 8192;  // J blocks per CTA: 32 KB of counters
+constexpr int kRareThreads = 512;
+constexpr int kRarePhase = 1024;      // J blocks whose records a CTA places at a time
+constexpr int kRareProgress = 8192;   // postings per row block with progress in shared memory
 
-// The records of the pairs posting k opens, at off[k].
-__global__ void k_rare_pairs(const uint64_t* __restrict__ keys, const uint32_t* __restrict__ vals,
-                             const int64_t* __restrict__ off, int64_t m, int rbits, int64_t nb,
-                             uint64_t* __restrict__ pkey, uint32_t* __restrict__ pval) {
+// CTA (I, y): the pairs whose first row lies in row block I and whose
+// second row's block J lies in [J0, J1) = [y kRareTileChunk, (y + 1)
+// kRareTileChunk) from J >= I on; the tiles (I, J) of the range are
+// consecutive in triangular order from tbase. Writes the range's record
+// counts to ex_off. A warp takes 32 postings at a time: their headers load
+// in one step, then the lanes run over each posting's pairs in turn.
+__global__ void __launch_bounds__(kRareThreads)
+    k_rare_tile_counts(const uint64_t* __restrict__ keys, const uint32_t* __restrict__ inv,
+                       const int32_t* __restrict__ cnt, const int64_t* __restrict__ rptr,
+                       int64_t n, int rbits, int64_t nb, uint32_t* __restrict__ ex_off) {
+  __shared__ uint32_t sm[kRareTileChunk];
+  const int64_t I = blockIdx.x;
+  const int64_t J0 = max(I, (int64_t)blockIdx.y * kRareTileChunk);
+  const int64_t J1 = min(nb, ((int64_t)blockIdx.y + 1) * kRareTileChunk);
+  if (J0 >= J1) return;  // the whole CTA: a range below the diagonal
+  const int nj = (int)(J1 - J0);
+  const int64_t tbase = tile_index(I, J0, nb);
+  for (int j = threadIdx.x; j < nj; j += blockDim.x) sm[j] = 0u;
+  __syncthreads();
   const uint64_t rmask = (1ull << rbits) - 1ull;
-  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < m;
-       k += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t cnt = off[k + 1] - off[k];
-    if (cnt == 0) continue;
-    const int64_t ra = (int64_t)(keys[k] & rmask);
-    const float ua = __uint_as_float(vals[k]);
-    const int64_t I = ra / kBlockRows;
-    for (int64_t q = 0; q < cnt; ++q) {
-      const int64_t rb = (int64_t)(keys[k + 1 + q] & rmask);  // rows ascend: ra < rb
-      const int64_t J = rb / kBlockRows;
-      pkey[off[k] + q] = (tri_tile(I, J, nb) << 14) | ((uint64_t)(ra % kBlockRows) << 7) |
-                         (uint64_t)(rb % kBlockRows);
-      pval[off[k] + q] = (uint32_t)tail_fixed(ua * __uint_as_float(vals[k + 1 + q]));
+  const int64_t rlo = J0 * kBlockRows, rhi = J1 * kBlockRows;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int64_t lo = rptr[I * kBlockRows], hi = rptr[min(n, (I + 1) * kBlockRows)];
+  for (int64_t i0 = lo + 32 * warp; i0 < hi; i0 += 32 * nw) {
+    uint32_t k = 0;
+    int c = 0;
+    if (i0 + lane < hi) {
+      k = inv[i0 + lane];
+      c = cnt[k];
+    }
+    unsigned todo = __ballot_sync(0xffffffffu, c > 0);
+    while (todo) {
+      const int src = __ffs(todo) - 1;
+      todo &= todo - 1;
+      const uint32_t kk = __shfl_sync(0xffffffffu, k, src);
+      const int cc = __shfl_sync(0xffffffffu, c, src);
+      for (int q = lane; q < cc; q += 32) {
+        const int64_t rb = (int64_t)(keys[kk + 1 + q] & rmask);
+        if (rb >= rlo && rb < rhi) atomicAdd(&sm[(int)(rb / kBlockRows - J0)], 1u);
+      }
     }
   }
+  __syncthreads();
+  for (int j = threadIdx.x; j < nj; j += blockDim.x) ex_off[tbase + j] = sm[j];
 }
 
-// off[t] = first record of tile t (records sorted by tile), t = 0 .. ntiles.
-__global__ void k_tile_starts(const uint64_t* __restrict__ pkey, int64_t m, int64_t ntiles,
-                              uint32_t* __restrict__ off) {
-  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k <= m;
-       k += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t prev = k == 0 ? -1 : (int64_t)(pkey[k - 1] >> 14);
-    const int64_t cur = k == m ? ntiles : (int64_t)(pkey[k] >> 14);
-    for (int64_t t = prev + 1; t <= cur; ++t) off[t] = (uint32_t)k;
+// First q in [0, c) whose row (keys[k + 1 + q]) is >= row_lo; c if none.
+__device__ __forceinline__ int first_row_at(const uint64_t* __restrict__ keys, uint32_t k, int c,
+                                            uint64_t rmask, int64_t row_lo) {
+  int lo = 0, hi = c;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if ((int64_t)(keys[k + 1 + mid] & rmask) < row_lo) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo;
+}
+
+// The same CTAs place every pair's record at its tile's shared-memory
+// cursor (ex_off holds the tiles' first records). They do so one phase of
+// kRarePhase J blocks at a time, so that the cursors being written at once,
+// over all CTAs, stay few enough for their partly written sectors to wait
+// in L2 until they are full. Each posting's progress (its first pair not
+// yet placed; rows ascend along a feature's postings) is kept in shared
+// memory, or found again by binary search in a block with more postings.
+__global__ void __launch_bounds__(kRareThreads)
+    k_rare_place(const uint64_t* __restrict__ keys, const uint32_t* __restrict__ vs,
+                 const uint32_t* __restrict__ inv, const int32_t* __restrict__ cnt,
+                 const int64_t* __restrict__ rptr, int64_t n, int rbits, int64_t nb,
+                 const uint32_t* __restrict__ ex_off, uint64_t* __restrict__ rec) {
+  __shared__ uint32_t cur[kRareTileChunk];
+  __shared__ uint16_t prog[kRareProgress];
+  const int64_t I = blockIdx.x;
+  const int64_t J0 = max(I, (int64_t)blockIdx.y * kRareTileChunk);
+  const int64_t J1 = min(nb, ((int64_t)blockIdx.y + 1) * kRareTileChunk);
+  if (J0 >= J1) return;  // the whole CTA: a range below the diagonal
+  const int nj = (int)(J1 - J0);
+  const int64_t tbase = tile_index(I, J0, nb);
+  for (int j = threadIdx.x; j < nj; j += blockDim.x) cur[j] = ex_off[tbase + j];
+  const uint64_t rmask = (1ull << rbits) - 1ull;
+  const int64_t lo = rptr[I * kBlockRows], hi = rptr[min(n, (I + 1) * kBlockRows)];
+  const bool keep = hi - lo <= kRareProgress;
+  if (keep) {
+    // a feature's later rows all lie past block I: only a range that starts
+    // above the diagonal skips some
+    for (int64_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+      const uint32_t k = inv[i];
+      const int c = cnt[k];
+      prog[i - lo] = (uint16_t)(J0 == I || c == 0 ? 0 : first_row_at(keys, k, c, rmask,
+                                                                        J0 * kBlockRows));
+    }
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int64_t P0 = J0; P0 < J1; P0 += kRarePhase) {
+    const int64_t rlo = P0 * kBlockRows, rhi = min(J1, P0 + kRarePhase) * kBlockRows;
+    // a warp keeps the same postings in every phase: their progress entries
+    // are read and written by the same lanes
+    for (int64_t i0 = lo + 32 * warp; i0 < hi; i0 += 32 * nw) {
+      uint32_t k = 0;
+      int c = 0, q0 = 0;
+      if (i0 + lane < hi) {
+        k = inv[i0 + lane];
+        c = cnt[k];
+        if (c > 0) q0 = keep ? (int)prog[i0 + lane - lo] : first_row_at(keys, k, c, rmask, rlo);
+      }
+      const bool live = q0 < c;
+      const int64_t ra = live ? (int64_t)(keys[k] & rmask) : 0;
+      const uint32_t ub = live ? vs[k] : 0u;
+      unsigned todo = __ballot_sync(0xffffffffu, live);
+      while (todo) {
+        const int src = __ffs(todo) - 1;
+        todo &= todo - 1;
+        const uint32_t kk = __shfl_sync(0xffffffffu, k, src);
+        const int cc = __shfl_sync(0xffffffffu, c, src);
+        const int qq = __shfl_sync(0xffffffffu, q0, src);
+        const int64_t rr = __shfl_sync(0xffffffffu, ra, src);
+        const float ua = __uint_as_float(__shfl_sync(0xffffffffu, ub, src));
+        int qend = cc;
+        for (int qb = qq; qb < cc; qb += 32) {
+          const int q = qb + lane;
+          bool in = false;
+          if (q < cc) {
+            const int64_t rb = (int64_t)(keys[kk + 1 + q] & rmask);  // >= rlo, ascending
+            in = rb < rhi;
+            if (in) {
+              const uint32_t at = atomicAdd(&cur[(int)(rb / kBlockRows - J0)], 1u);
+              const int prod = tail_fixed(ua * __uint_as_float(vs[kk + 1 + q]));
+              rec[at] = ((uint64_t)(uint32_t)prod << 32) | ((uint64_t)(rr % kBlockRows) << 7) |
+                        (uint64_t)(rb % kBlockRows);
+            }
+          }
+          // the lanes in the phase are a prefix: the first one out ends it
+          const unsigned b = __ballot_sync(0xffffffffu, in);
+          if (b != 0xffffffffu) {
+            qend = qb + __popc(b);
+            break;
+          }
+        }
+        if (keep && lane == src) prog[i0 + src - lo] = (uint16_t)qend;
+      }
+    }
   }
 }
 
@@ -837,40 +979,43 @@ cuapss_status build_explicit_pairs(Side& s, const PrepOptions& o, int64_t* rcoun
   const int rbits = std::max(1, bits_for((uint64_t)n));
   const int fbits = std::max(1, bits_for((uint64_t)(s.d - o.rare_from)));
   uint64_t* keys = nullptr;
-  uint32_t* vals = nullptr;
+  uint32_t *idx = nullptr, *vrm = nullptr, *vs = nullptr, *inv = nullptr;
+  int32_t* cnt = nullptr;
+  unsigned long long* total = nullptr;
   ST_TRY(ws.get(t + "rare:keys", (size_t)m, &keys));
-  ST_TRY(ws.get(t + "rare:vals", (size_t)m, &vals));
+  ST_TRY(ws.get(t + "rare:idx", (size_t)m, &idx));
+  ST_TRY(ws.get(t + "rare:vrm", (size_t)m, &vrm));
+  ST_TRY(ws.get(t + "rare:vs", (size_t)m, &vs));
+  ST_TRY(ws.get(t + "rare:inv", (size_t)m, &inv));
+  ST_TRY(ws.get(t + "rare:cnt", (size_t)m, &cnt));
+  ST_TRY(ws.get(t + "rare:total", 1, &total));
   k_rare_keys<<<grid_for(n * 32, kThreads), kThreads, 0, st>>>(s.rp2, s.col2, s.val2, rptr, n,
-                                                               o.rare_from, rbits, keys, vals);
+                                                               o.rare_from, rbits, keys, idx, vrm);
   LAUNCH_CHECK();
-  ST_TRY(radix_sort_pairs(keys, vals, m, rbits + fbits, ws, t + "rare", st));
-  int64_t* poff = nullptr;
-  ST_TRY(ws.get(t + "rare:poff", (size_t)m + 1, &poff));
+  ST_TRY(radix_sort_pairs(keys, idx, m, rbits + fbits, ws, t + "rare", st));
+  k_rare_gather<<<grid_for(m, kThreads), kThreads, 0, st>>>(idx, vrm, m, vs, inv);
+  LAUNCH_CHECK();
+  CU_TRY(cudaMemsetAsync(total, 0, sizeof(unsigned long long), st));
   k_rare_pair_counts<<<grid_for(m, kThreads), kThreads, 0, st>>>(keys, m, rbits,
-                                                                 o.rare_max_count, poff);
+                                                                 o.rare_max_count, cnt, total);
   LAUNCH_CHECK();
-  ST_TRY(exclusive_scan<int64_t>(poff, poff, m, poff + m, ws, t + "rare:pscan", st));
-  int64_t P = 0;
-  CU_TRY(cudaMemcpyAsync(&P, poff + m, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+  unsigned long long P = 0;
+  CU_TRY(cudaMemcpyAsync(&P, total, sizeof(P), cudaMemcpyDeviceToHost, st));
   CU_TRY(cudaStreamSynchronize(st));
-  if (P >= (int64_t)UINT32_MAX - 1) return CUAPSS_EINVAL;
-  s.n_explicit = P;
+  if (P >= (unsigned long long)UINT32_MAX - 1) return CUAPSS_EINVAL;
+  s.n_explicit = (int64_t)P;
   if (P == 0) {
     CU_TRY(cudaMemsetAsync(off, 0, sizeof(uint32_t) * (ntiles + 1), st));
     return CUAPSS_OK;
   }
-  uint64_t* pkey = nullptr;
-  uint32_t* pval = nullptr;
-  ST_TRY(ws.get(t + "ex_key", (size_t)P, &pkey));
-  ST_TRY(ws.get(t + "ex_val", (size_t)P, &pval));
-  k_rare_pairs<<<grid_for(m, kThreads), kThreads, 0, st>>>(keys, vals, poff, m, rbits, nb, pkey,
-                                                           pval);
+  ST_TRY(ws.get(t + "ex_rec", (size_t)P, &s.ex_rec));
+  const dim3 grid((unsigned)nb, (unsigned)((nb + kRareTileChunk - 1) / kRareTileChunk));
+  k_rare_tile_counts<<<grid, kRareThreads, 0, st>>>(keys, inv, cnt, rptr, n, rbits, nb, off);
   LAUNCH_CHECK();
-  ST_TRY(radix_sort_pairs(pkey, pval, P, bits_for((uint64_t)ntiles) + 14, ws, t + "ex", st));
-  k_tile_starts<<<grid_for(P + 1, kThreads), kThreads, 0, st>>>(pkey, P, ntiles, off);
+  ST_TRY(exclusive_scan<uint32_t>(off, off, ntiles, off + ntiles, ws, t + "ex_scan", st));
+  k_rare_place<<<grid, kRareThreads, 0, st>>>(keys, vs, inv, cnt, rptr, n, rbits, nb, off,
+                                              s.ex_rec);
   LAUNCH_CHECK();
-  s.ex_key = pkey;
-  s.ex_val = reinterpret_cast<int32_t*>(pval);
   return CUAPSS_OK;
 }
 
@@ -958,23 +1103,26 @@ cuapss_status feature_perm(const int32_t* counts, int64_t d, int64_t max_count, 
   return CUAPSS_OK;
 }
 
-// Rare-feature statistics for candidate thresholds C[k]: out[2k] = features
-// occurring in more than C[k] rows, out[2k + 1] = pairs of the tail features
-// (rank >= p) occurring in at most C[k] rows.
-constexpr int kRareCands = 4;
-__host__ __device__ constexpr int rare_cand(int k) { return 128 >> k; }  // 128, 64, 32, 16
+// Rare-feature statistics for candidate thresholds C[k]: out[3k] = features
+// occurring in more than C[k] rows, out[3k + 1] = pairs of the features
+// occurring in at most C[k] rows, out[3k + 2] = their postings.
+constexpr int kRareCands = 8;
+__host__ __device__ constexpr int rare_cand(int k) { return kMaxRareCount >> k; }  // 2048 .. 16
 
-__global__ void k_rare_stats(const int32_t* __restrict__ counts, const int32_t* __restrict__ perm,
-                             int64_t d, int p, unsigned long long* __restrict__ out) {
-  unsigned long long above[kRareCands] = {}, pairs[kRareCands] = {};
+__global__ void k_rare_stats(const int32_t* __restrict__ counts, int64_t d,
+                             unsigned long long* __restrict__ out) {
+  unsigned long long above[kRareCands] = {}, pairs[kRareCands] = {}, posts[kRareCands] = {};
   for (int64_t f = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; f < d;
        f += (int64_t)gridDim.x * blockDim.x) {
     const int64_t c = counts[f];
-    const bool tail = perm[f] >= p;
 #pragma unroll
     for (int k = 0; k < kRareCands; ++k) {
-      above[k] += c > rare_cand(k) ? 1ull : 0ull;
-      if (tail && c >= 2 && c <= rare_cand(k)) pairs[k] += (unsigned long long)(c * (c - 1) / 2);
+      if (c > rare_cand(k)) {
+        above[k] += 1ull;
+      } else {
+        pairs[k] += (unsigned long long)(c * (c - 1) / 2);
+        posts[k] += (unsigned long long)c;
+      }
     }
   }
 #pragma unroll
@@ -983,35 +1131,35 @@ __global__ void k_rare_stats(const int32_t* __restrict__ counts, const int32_t* 
     for (int o = 16; o > 0; o >>= 1) {
       above[k] += __shfl_xor_sync(0xffffffffu, above[k], o);
       pairs[k] += __shfl_xor_sync(0xffffffffu, pairs[k], o);
+      posts[k] += __shfl_xor_sync(0xffffffffu, posts[k], o);
     }
     if ((threadIdx.x & 31) == 0) {
-      atomicAdd(&out[2 * k], above[k]);
-      atomicAdd(&out[2 * k + 1], pairs[k]);
+      atomicAdd(&out[3 * k], above[k]);
+      atomicAdd(&out[3 * k + 1], pairs[k]);
+      atomicAdd(&out[3 * k + 2], posts[k]);
     }
   }
 }
 
-cuapss_status choose_rare_features(const int32_t* counts, const int32_t* perm, int64_t d, int p,
-                                   int64_t max_pairs, Workspace& ws, cudaStream_t st,
-                                   int64_t* rare_from, int* max_count) {
-  *rare_from = 0;
-  *max_count = 0;
+cuapss_status rare_feature_candidates(const int32_t* counts, int64_t d, Workspace& ws,
+                                      cudaStream_t st, std::vector<RareCandidate>* cands) {
+  cands->clear();
   unsigned long long* out = nullptr;
-  ST_TRY(ws.get("rare:stats", 2 * kRareCands, &out));
-  CU_TRY(cudaMemsetAsync(out, 0, sizeof(unsigned long long) * 2 * kRareCands, st));
-  k_rare_stats<<<grid_for(d, kThreads), kThreads, 0, st>>>(counts, perm, d, p, out);
+  ST_TRY(ws.get("rare:stats", 3 * kRareCands, &out));
+  CU_TRY(cudaMemsetAsync(out, 0, sizeof(unsigned long long) * 3 * kRareCands, st));
+  k_rare_stats<<<grid_for(d, kThreads), kThreads, 0, st>>>(counts, d, out);
   LAUNCH_CHECK();
-  unsigned long long h[2 * kRareCands];
+  unsigned long long h[3 * kRareCands];
   CU_TRY(cudaMemcpyAsync(h, out, sizeof(h), cudaMemcpyDeviceToHost, st));
   CU_TRY(cudaStreamSynchronize(st));
   for (int k = 0; k < kRareCands; ++k) {
-    if ((int64_t)h[2 * k + 1] <= max_pairs) {
-      // features of count <= C hold the ranks >= (features above C); the
-      // head keeps its p ranks in any case
-      *rare_from = std::max<int64_t>((int64_t)h[2 * k], p);
-      *max_count = rare_cand(k);
-      return CUAPSS_OK;
-    }
+    // the features of count <= C hold the ranks from (features above C) on
+    RareCandidate c;
+    c.max_count = rare_cand(k);
+    c.rank = (int64_t)h[3 * k];
+    c.pairs = (int64_t)h[3 * k + 1];
+    c.postings = (int64_t)h[3 * k + 2];
+    if (c.postings > 0) cands->push_back(c);
   }
   return CUAPSS_OK;
 }
@@ -1087,8 +1235,7 @@ cuapss_status build_side(Side& s, const PrepOptions& o, const int32_t* perm, Wor
   int64_t* rcount = nullptr;
   if (o.rare_from > 0) ST_TRY(ws.get(t + "rcount", (size_t)n + 1, &rcount));
   s.ex_off = nullptr;
-  s.ex_key = nullptr;
-  s.ex_val = nullptr;
+  s.ex_rec = nullptr;
   s.n_explicit = 0;
   ST_TRY(ws.get(t + "hlen", (size_t)n, &s.hlen));
   ST_TRY(ws.get(t + "nnzrow", (size_t)n, &s.nnz_row));

@@ -38,13 +38,19 @@ cuapss_status feature_perm(const int32_t* counts, int64_t d, int64_t max_count, 
 cuapss_status rank_count_prefix(const int32_t* counts, int64_t d, int remap, int64_t m,
                                 Workspace& ws, cudaStream_t st, std::vector<int64_t>* prefix);
 
-// Rare features of a self-join (explicit pairs instead of probes): the
-// largest threshold C in {128, 64, 32, 16} whose tail features occurring in
-// at most C rows give at most max_pairs pairs; *rare_from = the first rank
-// of those features (>= p), *max_count = C; both 0 when none qualifies.
-cuapss_status choose_rare_features(const int32_t* counts, const int32_t* perm, int64_t d, int p,
-                                   int64_t max_pairs, Workspace& ws, cudaStream_t st,
-                                   int64_t* rare_from, int* max_count);
+// Rare features of a self-join (explicit pairs instead of probes), for each
+// threshold C in {2048, 1024, ..., 16}: the features occurring in at most C
+// rows, which under the frequency remap hold the ranks from `rank` on, their
+// postings and their pairs. Thresholds with no such feature are left out.
+constexpr int kMaxRareCount = 2048;
+struct RareCandidate {
+  int max_count = 0;      // C
+  int64_t rank = 0;       // first rank of the features with count <= C
+  int64_t pairs = 0;      // sum of count (count - 1) / 2 over them
+  int64_t postings = 0;   // sum of count over them
+};
+cuapss_status rare_feature_candidates(const int32_t* counts, int64_t d, Workspace& ws,
+                                      cudaStream_t st, std::vector<RareCandidate>* cands);
 
 // Builds every array of `s` (s.rp0/col0/val0/n/d/nnz must be set).
 cuapss_status build_side(Side& s, const PrepOptions& o, const int32_t* perm, Workspace& ws,

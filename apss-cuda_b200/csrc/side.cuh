@@ -77,12 +77,11 @@ struct Side {
   int64_t max_block_tail = 0;
   std::vector<int64_t> h_bptr;    // host copy of bptr (unit scheduling)
   int64_t tail_products = 0;      // sum over tail lists of L(L-1)/2
-  // explicit pairs of the rare features (self-joins): records sorted by
-  // triangular tile index, {tile << 14 | row in I block << 7 | column in J
-  // block} with the fixed-point product; ex_off[t] = first record of tile t
+  // explicit pairs of the rare features (self-joins): records grouped by
+  // triangular tile index, {fixed-point product << 32 | row in I block << 7
+  // | column in J block}; ex_off[t] = first record of tile t
   uint32_t* ex_off = nullptr;
-  uint64_t* ex_key = nullptr;
-  int32_t* ex_val = nullptr;
+  uint64_t* ex_rec = nullptr;
   int64_t n_explicit = 0;
   double nrm_max = 1.0;           // largest row norm (FP64)
 };

@@ -150,10 +150,10 @@ __device__ __forceinline__ void tail_explicit(const TileArgs& A, uint32_t lo, ui
                                               int* acc, int ld, int cofs, int ncols, int tid,
                                               int nthreads) {
   for (uint32_t k = lo + (uint32_t)tid; k < hi; k += (uint32_t)nthreads) {
-    const uint64_t key = __ldg(&A.ex_key[k]);
-    const int c = (int)(key & 127u) - cofs;
+    const uint64_t rec = __ldg(&A.ex_rec[k]);
+    const int c = (int)(rec & 127u) - cofs;
     if (c >= 0 && c < ncols)
-      atomicAdd(acc + acc_cell<SWZ>((int)((key >> 7) & 127u), c, ld), __ldg(&A.ex_val[k]));
+      atomicAdd(acc + acc_cell<SWZ>((int)((rec >> 7) & 127u), c, ld), (int)(rec >> 32));
   }
 }
 

@@ -205,8 +205,9 @@ __device__ __forceinline__ void load_record(const TileArgs& A, uint32_t lo, uint
   rc = kNoRecord;
   rv = 0;
   if (lo + (uint32_t)tid < hi) {
-    rc = (uint32_t)(__ldg(&A.ex_key[lo + tid]) & 0x3fffu);
-    rv = __ldg(&A.ex_val[lo + tid]);
+    const uint64_t rec = __ldg(&A.ex_rec[lo + tid]);
+    rc = (uint32_t)rec & 0x3fffu;
+    rv = (int)(rec >> 32);
   }
 }
 

@@ -44,6 +44,7 @@ class Opts(ctypes.Structure):
         ("validate", ctypes.c_int),
         ("norm_tol", ctypes.c_float),
         ("verbose", ctypes.c_int),
+        ("rare_max_count", ctypes.c_int),
     ]
 
 
@@ -86,6 +87,8 @@ class Stats(ctypes.Structure):
         ("ms_finalize", ctypes.c_double),
         ("ms_total", ctypes.c_double),
         ("launches", ctypes.c_int64),
+        ("explicit_pairs", ctypes.c_int64),
+        ("rare_max_count", ctypes.c_int64),
     ]
 
     def as_dict(self) -> dict:
@@ -228,7 +231,7 @@ class Context:
 
     def __init__(self, device: int = 0, precision: int = PREC_FP32, head_width: int = 0,
                  remap: bool = True, validate: bool = True, norm_tol: float = 1e-4,
-                 stream: int | None = None):
+                 stream: int | None = None, rare_max_count: int = 0):
         o = default_opts()
         o.device = device
         o.precision = precision
@@ -237,6 +240,7 @@ class Context:
         o.validate = 1 if validate else 0
         o.norm_tol = norm_tol
         o.stream = stream
+        o.rare_max_count = rare_max_count
         self._h = _P()
         _check(lib().cuapss_create(ctypes.byref(self._h), ctypes.byref(o)), "cuapss_create")
         self.last_stats: dict = {}

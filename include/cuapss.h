@@ -70,6 +70,10 @@ typedef struct {
   int validate;        /* 1 (default): check CSR structure and row norms */
   float norm_tol;      /* accepted | ||x||_2 - 1 | (default 1e-4) */
   int verbose;         /* reserved, 0 */
+  int rare_max_count;  /* self-joins: features occurring in at most C rows
+                          have their pairs enumerated instead of probed.
+                          0 (default): C chosen with p by the cost model;
+                          -1: none; C in {16, 32, ..., 2048}: that C */
 } cuapss_opts;
 
 typedef struct {
@@ -106,6 +110,9 @@ typedef struct {
   double ms_finalize;     /* rescore, compensated re-score, sort, copy-out */
   double ms_total;
   int64_t launches;       /* CUDA kernels this call launched */
+  int64_t explicit_pairs; /* rare-feature pairs enumerated instead of probed */
+  int64_t rare_max_count; /* their features occur in at most this many rows
+                             (0: every tail feature probed) */
 } cuapss_stats;
 
 typedef struct cuapss_ctx cuapss_ctx;

@@ -56,6 +56,7 @@ def test_status_strings_and_defaults():
     o = cuapss.default_opts()
     assert o.remap == 1 and o.validate == 1 and o.precision == cuapss.PREC_FP32
     assert abs(o.norm_tol - 1e-4) < 1e-9
+    assert o.rare_max_count == 0
 
 
 def test_create_without_device_fails_cleanly():
@@ -74,6 +75,11 @@ def test_bad_options_rejected():
     o.precision = 7
     assert cuapss.lib().cuapss_create(ctypes.byref(h), ctypes.byref(o)) == cuapss.EINVAL
     assert cuapss.lib().cuapss_create(None, None) == cuapss.EINVAL
+    # the rare-feature threshold: -1, 0 or a power of two in 16 .. 2048
+    for bad in (-2, 8, 24, 4096):
+        o = cuapss.default_opts()
+        o.rare_max_count = bad
+        assert cuapss.lib().cuapss_create(ctypes.byref(h), ctypes.byref(o)) == cuapss.EINVAL
 
 
 def test_synth_determinism_and_shape():
