@@ -871,6 +871,24 @@ __device__ __forceinline__ int first_row_at(const uint64_t* __restrict__ keys, u
   return lo;
 }
 
+constexpr int kPlaceBatch = 4;  // postings whose first pairs load together
+
+// Record of one pair (second posting key / value bits) at its tile's
+// cursor, if the pair is valid and its second row lies below rhi (rows at
+// or past rhi belong to a later phase). Returns whether it was placed.
+__device__ __forceinline__ bool place_pair(bool valid, uint64_t key, uint32_t vbits, int64_t ra,
+                                           float ua, uint64_t rmask, int64_t rhi, int64_t J0,
+                                           uint32_t* cur, uint64_t* __restrict__ rec) {
+  if (!valid) return false;
+  const int64_t rb = (int64_t)(key & rmask);  // >= the phase's first row, ascending
+  if (rb >= rhi) return false;
+  const uint32_t at = atomicAdd(&cur[(int)(rb / kBlockRows - J0)], 1u);
+  const int prod = tail_fixed(ua * __uint_as_float(vbits));
+  rec[at] = ((uint64_t)(uint32_t)prod << 32) | ((uint64_t)(ra % kBlockRows) << 7) |
+            (uint64_t)(rb % kBlockRows);
+  return true;
+}
+
 // The same CTAs place every pair's record at its tile's shared-memory
 // cursor (ex_off holds the tiles' first records). They do so one phase of
 // kRarePhase J blocks at a time, so that the cursors being written at once,
@@ -924,35 +942,50 @@ __global__ void __launch_bounds__(kRareThreads)
       const uint32_t ub = live ? vs[k] : 0u;
       unsigned todo = __ballot_sync(0xffffffffu, live);
       while (todo) {
-        const int src = __ffs(todo) - 1;
-        todo &= todo - 1;
-        const uint32_t kk = __shfl_sync(0xffffffffu, k, src);
-        const int cc = __shfl_sync(0xffffffffu, c, src);
-        const int qq = __shfl_sync(0xffffffffu, q0, src);
-        const int64_t rr = __shfl_sync(0xffffffffu, ra, src);
-        const float ua = __uint_as_float(__shfl_sync(0xffffffffu, ub, src));
-        int qend = cc;
-        for (int qb = qq; qb < cc; qb += 32) {
-          const int q = qb + lane;
-          bool in = false;
-          if (q < cc) {
-            const int64_t rb = (int64_t)(keys[kk + 1 + q] & rmask);  // >= rlo, ascending
-            in = rb < rhi;
-            if (in) {
-              const uint32_t at = atomicAdd(&cur[(int)(rb / kBlockRows - J0)], 1u);
-              const int prod = tail_fixed(ua * __uint_as_float(vs[kk + 1 + q]));
-              rec[at] = ((uint64_t)(uint32_t)prod << 32) | ((uint64_t)(rr % kBlockRows) << 7) |
-                        (uint64_t)(rb % kBlockRows);
-            }
-          }
-          // the lanes in the phase are a prefix: the first one out ends it
-          const unsigned b = __ballot_sync(0xffffffffu, in);
-          if (b != 0xffffffffu) {
-            qend = qb + __popc(b);
-            break;
-          }
+        // kPlaceBatch postings at a time: the keys and values of their first
+        // 32 pairs load together, so their latencies overlap
+        int src[kPlaceBatch];
+#pragma unroll
+        for (int j = 0; j < kPlaceBatch; ++j) {
+          src[j] = todo ? __ffs(todo) - 1 : -1;
+          todo &= todo - 1;
         }
-        if (keep && lane == src) prog[i0 + src - lo] = (uint16_t)qend;
+        uint32_t kk[kPlaceBatch], vb[kPlaceBatch];
+        int cc[kPlaceBatch], qq[kPlaceBatch];
+        int64_t rr[kPlaceBatch];
+        float ua[kPlaceBatch];
+        uint64_t kb[kPlaceBatch];
+#pragma unroll
+        for (int j = 0; j < kPlaceBatch; ++j) {
+          const int sj = src[j] < 0 ? 0 : src[j];
+          kk[j] = __shfl_sync(0xffffffffu, k, sj);
+          cc[j] = src[j] < 0 ? 0 : __shfl_sync(0xffffffffu, c, sj);
+          qq[j] = __shfl_sync(0xffffffffu, q0, sj);
+          rr[j] = __shfl_sync(0xffffffffu, ra, sj);
+          ua[j] = __uint_as_float(__shfl_sync(0xffffffffu, ub, sj));
+          const int q = qq[j] + lane;
+          kb[j] = q < cc[j] ? keys[kk[j] + 1 + q] : 0ull;
+          vb[j] = q < cc[j] ? vs[kk[j] + 1 + q] : 0u;
+        }
+#pragma unroll
+        for (int j = 0; j < kPlaceBatch; ++j) {
+          if (src[j] < 0) break;  // warp-uniform
+          // the lanes in the phase are a prefix: the first one out ends it
+          unsigned bm = __ballot_sync(0xffffffffu, place_pair(qq[j] + lane < cc[j], kb[j], vb[j],
+                                                              rr[j], ua[j], rmask, rhi, J0, cur,
+                                                              rec));
+          int qend = bm != 0xffffffffu ? qq[j] + __popc(bm) : cc[j];
+          for (int qb = qq[j] + 32; bm == 0xffffffffu && qb < cc[j]; qb += 32) {
+            const int q = qb + lane;
+            const bool v = q < cc[j];
+            bm = __ballot_sync(0xffffffffu,
+                               place_pair(v, v ? keys[kk[j] + 1 + q] : 0ull,
+                                          v ? vs[kk[j] + 1 + q] : 0u, rr[j], ua[j], rmask, rhi,
+                                          J0, cur, rec));
+            if (bm != 0xffffffffu) qend = qb + __popc(bm);
+          }
+          if (keep && lane == src[j]) prog[i0 + src[j] - lo] = (uint16_t)qend;
+        }
       }
     }
   }

@@ -477,6 +477,8 @@ def run_selfjoin(args, rank, world, local):
         "config": {"workload": workload, "n": x.n, "d": x.d, "nnz": x.nnz, "t": args.t,
                    "precision": args.precision, "head_width": p,
                    "named_head_width": NAMED_HEAD.get(workload),
+                   "rare_max_count": int(s0["rare_max_count"]),
+                   "explicit_pairs": int(s0["explicit_pairs"]),
                    "l2": "inputs larger than L2 (CSR and head block are GBs)",
                    "parallelism": f"row-block shards x{world}" if world > 1 else "1 GPU"},
         "pairs_found": npairs, "candidates": s0["candidates"], "rescored": s0["rescored"],
