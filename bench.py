@@ -341,10 +341,11 @@ def tile_roofline(stats, p, pairs, n, world, prec_mixed, x, peaks_):
 
 # DRAM bytes (read + write) of k_tiles_mma per 128 x 128 tile and 64 head
 # features, from the ncu launch list of the n = d = 1M workload's shape at
-# 200,000 rows (137.0 GB over 1,222,266 tiles at p = 960; the full-size launch
-# is too large to capture). Scaled by tiles x p / 64; at full size the head
-# block is a larger multiple of the L2, so the true figure is higher.
-TILE_TRAFFIC_PER_CHUNK = 137.0e9 / 1_222_266 / 15
+# 200,000 rows (10.39 GB over 1,222,266 tiles at p = 960; the full-size launch
+# is too large to capture with several metrics). Scaled by tiles x p / 64; at
+# full size the head block is a larger multiple of the L2, so the true figure
+# may be higher.
+TILE_TRAFFIC_PER_CHUNK = 10.39e9 / 1_222_266 / 15
 
 
 def dry_shards(args, rank, world):
