@@ -125,6 +125,18 @@ int choose_head_width(int precision, int64_t n, int64_t d, int64_t nnz,
   return best_head_width(n, nnz, prefix, rare_rank, rare_postings, &cost);
 }
 
+bool head_bound_plan(int64_t p, int64_t n, int64_t nnz, const std::vector<int64_t>& prefix,
+                     const RareCandidate& rare) {
+  if (n <= 0 || prefix.size() < 2) return false;
+  const bool paired = rare.max_count > 0;
+  const TileCostModel& m = paired ? kRarePaired : kProbedTail;
+  const int64_t probed =
+      probed_postings(p, nnz, prefix, paired ? rare.rank : 0, paired ? rare.postings : 0);
+  const double head = m.head_chunk_ns * (double)(p / 64);
+  const double tail = m.tail_posting_ns * kBlockRows * ((double)probed / (double)n);
+  return head >= 2.0 * tail;
+}
+
 TilePlan plan_tiles(int precision, int64_t n, int64_t d, int64_t nnz,
                     const std::vector<int64_t>& prefix,
                     const std::vector<RareCandidate>& cands, int64_t max_pairs, int fixed_p,
@@ -256,7 +268,7 @@ cuapss_status join_device(cuapss_ctx* ctx, const DevCsr& a, const DevCsr* b, flo
   }
   const int64_t n_all = a.n + (self ? 0 : bb.n), nnz_all = a.nnz + (self ? 0 : bb.nnz);
   std::vector<int64_t> prefix;
-  if ((precision == CUAPSS_PREC_MIXED && ctx->opts.head_width <= 0) || !rare.empty())
+  if (precision == CUAPSS_PREC_MIXED || !rare.empty())
     ST_TRY(rank_count_prefix(counts, d, ctx->opts.remap, kMaxModelHead, ws, st, &prefix));
   int64_t max_pairs = 0;
   if (!rare.empty()) {
@@ -289,6 +301,7 @@ cuapss_status join_device(cuapss_ctx* ctx, const DevCsr& a, const DevCsr* b, flo
     po.rare_from = std::max<int64_t>(plan.rare.rank, p);
     po.rare_max_count = plan.rare.max_count;
   }
+  const bool head_bound = mixed && head_bound_plan(p, n_all, nnz_all, prefix, plan.rare);
   Side SA, SB;
   SA.rp0 = a.rp;
   SA.col0 = a.col;
@@ -395,7 +408,8 @@ cuapss_status join_device(cuapss_ctx* ctx, const DevCsr& a, const DevCsr* b, flo
     CU_TRY(cudaMemsetAsync(err, 0, sizeof(int), st));
     CU_TRY(cudaMemsetAsync(ccount, 0, sizeof(unsigned long long), st));
     if (ntiles > 0) {
-      if (mixed) ST_TRY(launch_tiles_mma(ta, SA.head16, SJ->head16, SA.p, grid, st));
+      if (mixed)
+        ST_TRY(launch_tiles_mma(ta, SA.head16, SJ->head16, SA.p, grid, st, false, head_bound));
       else ST_TRY(launch_tiles_fp32(ta, grid, st));
     }
     unsigned long long hc = 0;

@@ -56,6 +56,11 @@ int choose_head_width(int precision, int64_t n, int64_t d, int64_t nnz,
                       const std::vector<int64_t>& prefix, int64_t rare_rank = 0,
                       int64_t rare_postings = 0);
 
+// Whether the tile cost model puts the head at p at least twice the tail
+// still probed (the tile kernel's two-J-block MMA tiles then pay).
+bool head_bound_plan(int64_t p, int64_t n, int64_t nnz, const std::vector<int64_t>& prefix,
+                     const RareCandidate& rare);
+
 // Head width and rare-feature threshold of a self-join, chosen together by
 // the tile cost model: the threshold (of cands, at most max_pairs pairs, or
 // none) and p that minimise the modelled tile time plus the explicit pairs'

@@ -69,7 +69,10 @@ constexpr int kSlabs = kJSegs;                // slabs per tile
 constexpr int kSlabInts = kBlockRows * kSlabCols;  // one slab accumulator
 constexpr int kEpiCols = kSlabCols / (kEW / 4);    // slab columns per epilogue thread
 static_assert(kEpiCols == 16 || kEpiCols == 32, "tensor-memory loads of 16 or 32 columns");
-constexpr uint32_t kTmemCols = 256;
+// Tensor-memory columns of a variant whose MMA tiles span JW J blocks: two
+// accumulators of 128 x (128 JW) FP32.
+template <int JW>
+__host__ __device__ constexpr uint32_t tmem_cols() { return 256u * JW; }
 constexpr int kTailBar = 1;
 constexpr int kEpiBar = 2;
 constexpr int kBatch = 2;                     // J postings per thread per load batch
@@ -78,7 +81,7 @@ constexpr int kUnitReaders = 1 + kTW + kEW;   // MMA thread + tail warps + epilo
 static_assert(kSlabCols == 32, "slab accumulator rows are 32 ints (8 swizzled groups)");
 
 struct SmemM {
-  uint8_t* stage;       // STAGES x (A 16 KB | B 16 KB), 1024-byte aligned
+  uint8_t* stage;       // STAGES x (A 16 KB | B JW x 16 KB), 1024-byte aligned
   int* acc;             // [2][128][32] slab accumulators (swizzled groups)
   float* hnj;           // [2][128] per-column head margins of a tile
   uint64_t* full;
@@ -98,12 +101,13 @@ struct SmemM {
 
 __host__ __device__ constexpr size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
-// Shared-memory layout of the variant with STAGES operand stages and CAP
-// staged tail postings.
-template <int STAGES, int CAP>
+// Shared-memory layout of the variant with STAGES operand stages of an I
+// chunk and JW J chunks, and CAP staged tail postings.
+template <int STAGES, int CAP, int JW>
 struct Cfg {
   static constexpr int kBars = 2 * STAGES + 2 + 2 + 2 + 2 + 1 + 2 * kUnitRing;
-  static constexpr size_t kAcc = (size_t)STAGES * 2 * kTileBytes;
+  static constexpr size_t kStageBytes = (size_t)(1 + JW) * kTileBytes;
+  static constexpr size_t kAcc = (size_t)STAGES * kStageBytes;
   static constexpr size_t kHnj = align_up(kAcc + (size_t)2 * kSlabInts * 4, 16);
   static constexpr size_t kBar = align_up(kHnj + (size_t)2 * kBlockRows * 4, 16);
   static constexpr size_t kRing = align_up(kBar + (size_t)kBars * 8, 16);
@@ -115,9 +119,9 @@ struct Cfg {
   static_assert(kSmem <= 232448, "shared memory budget");
 };
 
-template <int STAGES, int CAP>
+template <int STAGES, int CAP, int JW>
 __device__ __forceinline__ SmemM carve(uint8_t* raw) {
-  using C = Cfg<STAGES, CAP>;
+  using C = Cfg<STAGES, CAP, JW>;
   uint8_t* base = reinterpret_cast<uint8_t*>(align_up(reinterpret_cast<size_t>(raw), 1024));
   SmemM s;
   s.stage = base;
@@ -230,10 +234,11 @@ struct MmaArgs {
   int nkc;  // p / 64
 };
 
-template <int STAGES, int CAP>
+template <int STAGES, int CAP, int JW>
 __global__ void __launch_bounds__(kThreads, 1) k_tiles_mma(const TileArgs A, const MmaArgs M) {
   extern __shared__ uint8_t smem_raw[];
-  const SmemM S = carve<STAGES, CAP>(smem_raw);
+  const SmemM S = carve<STAGES, CAP, JW>(smem_raw);
+  constexpr size_t kStageBytes = Cfg<STAGES, CAP, JW>::kStageBytes;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   volatile int* abort = S.abort;
   if (threadIdx.x == 0) {
@@ -256,7 +261,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_tiles_mma(const TileArgs A, con
     fence_mbar_init();
   }
   if (warp == 1) {
-    tmem_alloc(S.tmem_base, kTmemCols);
+    tmem_alloc(S.tmem_base, tmem_cols<JW>());
     tmem_relinquish();
   }
   if (warp >= 2)
@@ -286,7 +291,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_tiles_mma(const TileArgs A, con
         if (u >= A.nunits) break;
         const int4 U = A.units[u];
         if (U.y >= U.z) continue;
-        for (int J = U.y; ok && J < U.z; ++J) {
+        for (int J = U.y; ok && J < U.z; J += JW) {
+          const int w = U.z - J < JW ? U.z - J : JW;  // J blocks of this MMA tile
           for (int kc = 0; kc < M.nkc; ++kc, ++it) {
             const uint32_t s = it % STAGES, round = it / STAGES;
             if (!wait_or_abort(&S.empty[s], (round & 1u) ^ 1u, abort)) {
@@ -294,10 +300,14 @@ __global__ void __launch_bounds__(kThreads, 1) k_tiles_mma(const TileArgs A, con
               ok = false;
               break;
             }
-            uint8_t* dst = S.stage + (size_t)s * 2 * kTileBytes;
-            mbar_arrive_expect_tx(&S.full[s], 2 * kTileBytes);
+            uint8_t* dst = S.stage + (size_t)s * kStageBytes;
+            mbar_arrive_expect_tx(&S.full[s], (uint32_t)(1 + w) * kTileBytes);
             bulk_g2s(dst, M.headI16 + ((size_t)U.x * M.nkc + kc) * kTileBytes, kTileBytes,
                      &S.full[s]);
+            if (w == 2)  // the second J block's rows follow the first's
+              bulk_g2s(dst + 2 * kTileBytes,
+                       M.headJ16 + ((size_t)(J + 1) * M.nkc + kc) * kTileBytes, kTileBytes,
+                       &S.full[s]);
             bulk_g2s(dst + kTileBytes, M.headJ16 + ((size_t)J * M.nkc + kc) * kTileBytes,
                      kTileBytes, &S.full[s]);
           }
@@ -312,7 +322,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_tiles_mma(const TileArgs A, con
   } else if (warp == 1) {
     // ----------------------------------------------------------------- MMA
     if (lane == 0) {
-      const uint32_t idesc = umma_idesc_bf16(kBlockRows, kBlockRows);
+      // N = 128 w: one MMA tile spans w <= JW J blocks
+      const uint32_t idesc1 = umma_idesc_bf16(kBlockRows, kBlockRows);
+      const uint32_t idesc2 = umma_idesc_bf16(kBlockRows, 2 * kBlockRows);
       uint32_t it = 0, tt = 0;
       bool ok = true;
       for (uint32_t k = 0; ok; ++k) {
@@ -326,7 +338,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_tiles_mma(const TileArgs A, con
         if (u >= A.nunits) break;
         const int4 U = A.units[u];
         if (U.y >= U.z) continue;
-        for (int J = U.y; ok && J < U.z; ++J, ++tt) {
+        for (int J = U.y; ok && J < U.z; J += JW, ++tt) {
+          const int w = U.z - J < JW ? U.z - J : JW;
+          const uint32_t idesc = w == 2 ? idesc2 : idesc1;
           const uint32_t b = tt & 1u, tround = tt >> 1;
           if (!wait_or_abort(&S.tempty[b], (tround & 1u) ^ 1u, abort)) {
             raise_abort(A, abort);
@@ -334,7 +348,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_tiles_mma(const TileArgs A, con
             break;
           }
           tc_fence_after();
-          const uint32_t d = tmem + b * (uint32_t)kBlockRows;
+          const uint32_t d = tmem + b * (uint32_t)(kBlockRows * JW);
           for (int kc = 0; kc < M.nkc; ++kc, ++it) {
             const uint32_t s = it % STAGES, round = it / STAGES;
             if (!wait_or_abort(&S.full[s], round & 1u, abort)) {
@@ -343,7 +357,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_tiles_mma(const TileArgs A, con
               break;
             }
             tc_fence_after();
-            const uint8_t* st = S.stage + (size_t)s * 2 * kTileBytes;
+            const uint8_t* st = S.stage + (size_t)s * kStageBytes;
             const uint64_t ad = umma_desc_sw128(st);
             const uint64_t bd = umma_desc_sw128(st + kTileBytes);
 #pragma unroll
@@ -464,7 +478,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_tiles_mma(const TileArgs A, con
     const int colh = ew >> 2;        // which kEpiCols columns of each slab
     const int row = 32 * q4 + lane;  // tile row of this thread
     bool live = true;
-    uint32_t tt = 0, g = 0;
+    uint32_t tt = 0, g = 0, mt = 0;  // J tiles, slabs, MMA tiles of this CTA
     for (uint32_t ku = 0;; ++ku) {
       const uint32_t slot = ku % kUnitRing, ur = ku / kUnitRing;
       live = warp_wait(A, &S.ufull[slot], ur & 1u, abort, live);
@@ -481,7 +495,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_tiles_mma(const TileArgs A, con
       const float hn_r = row_ok ? A.hnormI[row0 + row] : 0.0f;
       const double t_r = A.t_row ? (row_ok ? (double)A.t_row[row0 + row] : 2.0) : (double)A.t;
       for (int J = U.y; J < U.z; ++J, ++tt) {
-        const uint32_t b = tt & 1u, tround = tt >> 1;
+        // J block jj of MMA tile mt (which spans up to JW J blocks)
+        const int jj = (J - U.y) % JW;
+        const bool mt_last = jj == JW - 1 || J + 1 == U.z;
+        const uint32_t b = mt & 1u, tround = mt >> 1;
         const int64_t col0 = (int64_t)J * kBlockRows;
         const int colsJ = (int)(A.nJ - col0 < kBlockRows ? A.nJ - col0 : kBlockRows);
         const bool diag = A.self && (I == J);
@@ -493,8 +510,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_tiles_mma(const TileArgs A, con
           hnj[etid] =
               etid < colsJ ? __double2float_ru(A.eps_head * (double)A.hnormJ[col0 + etid]) : 0.0f;
         named_bar(kEpiBar, kET);
-        live = warp_wait(A, &S.tfull[b], tround & 1u, abort, live);
-        tc_fence_after();
+        if (jj == 0) {
+          live = warp_wait(A, &S.tfull[b], tround & 1u, abort, live);
+          tc_fence_after();
+        }
         for (int q = 0; q < kSlabs; ++q, ++g) {
           const uint32_t k = g & 1u, use = g >> 1;
           live = warp_wait(A, &S.afull[k], use & 1u, abort, live);
@@ -502,8 +521,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_tiles_mma(const TileArgs A, con
             // ---- head (tensor memory) + tail (slab accumulator) vs t - eps
             const int cbase = q * kSlabCols + colh * kEpiCols;  // first tile column
             uint32_t v[kEpiCols];
-            const uint32_t taddr =
-                tmem + b * (uint32_t)kBlockRows + (uint32_t)cbase + ((uint32_t)(32 * q4) << 16);
+            const uint32_t taddr = tmem + b * (uint32_t)(kBlockRows * JW) +
+                                   (uint32_t)(jj * kBlockRows + cbase) +
+                                   ((uint32_t)(32 * q4) << 16);
             tmem_ld(taddr, v);
             int* arow = S.acc + k * kSlabInts + row * kSlabCols;
             const float4* hn4 = reinterpret_cast<const float4*>(hnj + cbase);
@@ -558,9 +578,12 @@ __global__ void __launch_bounds__(kThreads, 1) k_tiles_mma(const TileArgs A, con
           __syncwarp();
           if (live && lane == 0) mbar_arrive(&S.aempty[k]);
         }
-        tc_fence_before();
-        __syncwarp();
-        if (live && lane == 0) mbar_arrive(&S.tempty[b]);
+        if (mt_last) {
+          tc_fence_before();
+          __syncwarp();
+          if (live && lane == 0) mbar_arrive(&S.tempty[b]);
+          ++mt;
+        }
       }
     }
   }
@@ -568,16 +591,35 @@ __global__ void __launch_bounds__(kThreads, 1) k_tiles_mma(const TileArgs A, con
   __syncthreads();
   if (warp == 1) {
     tc_fence_after();
-    tmem_dealloc(tmem, kTmemCols);
+    tmem_dealloc(tmem, tmem_cols<JW>());
   }
 }
 
 }  // namespace
 
-// Kernel variants: more operand stages in flight when the I blocks' tails
-// fit a smaller staging area (most inputs), the large staging area otherwise.
-constexpr int kBigStages = 3, kBigCap = 12768;
+// Kernel variants, by the largest I block tail (staged postings) and whether
+// the caller's plan is head-bound:
+//   wide   MMA tiles of two J blocks (N = 256) over 3 stages of 48 KB: the I
+//          chunk is read once per two J blocks, 24 KB of operands per
+//          128 x 128 tile instead of 32 KB, 144 KB in flight; staging for
+//          5,936 tail postings;
+//   small  one J block per MMA tile, 4 stages of 32 KB, 7,936 postings;
+//   big    one J block per MMA tile, 3 stages, 12,768 postings.
+// The operand stream runs near the L2's bandwidth, so the wide variant, which
+// needs fewer bytes per tile, wins where the head sets the pace (measured at
+// n = 200,000 of the n = d = 1M shape: p = 1,536 58.3 ms against 72.6 ms).
+// Where the tail sets the pace it loses 6-7% (n = 400,000 and 1M, p = 1,024),
+// so the caller asks for it only for head-bound plans.
+constexpr int kWideStages = 3, kWideCap = 5936;
 constexpr int kSmallStages = 4, kSmallCap = 7936;
+constexpr int kBigStages = 3, kBigCap = 12768;
+
+template <int STAGES, int CAP, int JW>
+cudaError_t set_smem_attr() {
+  return cudaFuncSetAttribute(k_tiles_mma<STAGES, CAP, JW>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)Cfg<STAGES, CAP, JW>::kSmem);
+}
 
 // Opts the kernels into their dynamic shared memory once per device (outside
 // any stream capture when called ahead of it).
@@ -588,42 +630,47 @@ cuapss_status tiles_mma_init() {
   CU_TRY(cudaGetDevice(&dev));
   std::lock_guard<std::mutex> lk(mu);
   if (dev < 64 && ((done >> dev) & 1ull)) return CUAPSS_OK;
-  CU_TRY(cudaFuncSetAttribute(k_tiles_mma<kBigStages, kBigCap>,
-                              cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)Cfg<kBigStages, kBigCap>::kSmem));
-  CU_TRY(cudaFuncSetAttribute(k_tiles_mma<kSmallStages, kSmallCap>,
-                              cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)Cfg<kSmallStages, kSmallCap>::kSmem));
+  CU_TRY((set_smem_attr<kWideStages, kWideCap, 2>()));
+  CU_TRY((set_smem_attr<kSmallStages, kSmallCap, 1>()));
+  CU_TRY((set_smem_attr<kBigStages, kBigCap, 1>()));
   if (dev < 64) done |= 1ull << dev;
   return CUAPSS_OK;
 }
 
 cuapss_status launch_tiles_mma(const TileArgs& a, const void* headI16, const void* headJ16,
-                               int p, int grid, cudaStream_t st, bool overlap_prev) {
+                               int p, int grid, cudaStream_t st, bool overlap_prev,
+                               bool head_bound) {
   ST_TRY(tiles_mma_init());
   if (p <= 0 || p % kKC != 0) return CUAPSS_EINVAL;
   MmaArgs m;
   m.headI16 = static_cast<const uint8_t*>(headI16);
   m.headJ16 = static_cast<const uint8_t*>(headJ16);
   m.nkc = p / kKC;
-  const bool small = a.max_tailI <= kSmallCap;
+  const int variant = head_bound && a.max_tailI <= kWideCap ? 0
+                      : a.max_tailI <= kSmallCap            ? 1
+                                                            : 2;
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3((unsigned)grid);
   cfg.blockDim = dim3(kThreads);
-  cfg.dynamicSmemBytes =
-      small ? Cfg<kSmallStages, kSmallCap>::kSmem : Cfg<kBigStages, kBigCap>::kSmem;
+  cfg.dynamicSmemBytes = variant == 0   ? Cfg<kWideStages, kWideCap, 2>::kSmem
+                         : variant == 1 ? Cfg<kSmallStages, kSmallCap, 1>::kSmem
+                                        : Cfg<kBigStages, kBigCap, 1>::kSmem;
   cfg.stream = st;
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
   attr[0].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = attr;
   cfg.numAttrs = overlap_prev ? 1 : 0;
-  if (small) CU_TRY(cudaLaunchKernelEx(&cfg, k_tiles_mma<kSmallStages, kSmallCap>, a, m));
-  else CU_TRY(cudaLaunchKernelEx(&cfg, k_tiles_mma<kBigStages, kBigCap>, a, m));
+  if (variant == 0)
+    CU_TRY(cudaLaunchKernelEx(&cfg, k_tiles_mma<kWideStages, kWideCap, 2>, a, m));
+  else if (variant == 1)
+    CU_TRY(cudaLaunchKernelEx(&cfg, k_tiles_mma<kSmallStages, kSmallCap, 1>, a, m));
+  else
+    CU_TRY(cudaLaunchKernelEx(&cfg, k_tiles_mma<kBigStages, kBigCap, 1>, a, m));
   LAUNCH_CHECK();
   return CUAPSS_OK;
 }
 
-size_t tiles_mma_smem_bytes() { return Cfg<kBigStages, kBigCap>::kSmem; }
+size_t tiles_mma_smem_bytes() { return Cfg<kBigStages, kBigCap, 1>::kSmem; }
 
 }  // namespace cuapss

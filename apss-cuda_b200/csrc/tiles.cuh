@@ -106,9 +106,13 @@ int tiles_fp32_max_grid();
 
 // Mixed-precision tile kernel (BF16 head on tcgen05 tensor cores, FP32 tail).
 // headI16 / headJ16: BF16 head blocks in the swizzled layout of
-// build_side; p a multiple of 64.
+// build_side; p a multiple of 64. head_bound: the head's operand stream
+// dominates the tiles (the caller's cost model puts the head at least twice
+// the tail), so MMA tiles of two J blocks are used where the tail staging
+// fits them.
 cuapss_status launch_tiles_mma(const TileArgs& a, const void* headI16, const void* headJ16,
-                               int p, int grid, cudaStream_t st, bool overlap_prev = false);
+                               int p, int grid, cudaStream_t st, bool overlap_prev = false,
+                               bool head_bound = false);
 size_t tiles_mma_smem_bytes();
 cuapss_status tiles_mma_init();
 
