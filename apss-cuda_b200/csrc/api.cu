@@ -63,6 +63,10 @@ constexpr double kExplicitPairBytes = 8.0, kExplicitMemShare = 0.4;
 // kernel (about 4) and its share of the build's count and placement passes
 // (about 3.5), measured on the n = d = 1M workload's shape.
 constexpr double kExplicitPairSmNs = 7.5;
+// The tile kernel that adds explicit records holds them in registers and so
+// loads J postings two at a time instead of three: 7% slower per tile at
+// equal work (n = 800k, d = 50k: 1,017 against 945 ms with few records).
+constexpr double kExplicitKernelFactor = 1.07;
 
 struct TileCostModel {
   double head_chunk_ns, tail_posting_ns, overlap_loss;
@@ -157,6 +161,7 @@ TilePlan plan_tiles(int precision, int64_t n, int64_t d, int64_t nnz,
       per_tile = tile_ns(precision, p, n, probed_postings(p, nnz, prefix, rank, posts), c != nullptr);
     }
     *p_out = p;
+    if (c) per_tile *= kExplicitKernelFactor;
     return tiles * per_tile + (c ? (double)c->pairs * kExplicitPairSmNs : 0.0);
   };
   int p0 = plan.p;

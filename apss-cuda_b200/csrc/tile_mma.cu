@@ -75,7 +75,10 @@ template <int JW>
 __host__ __device__ constexpr uint32_t tmem_cols() { return 256u * JW; }
 constexpr int kTailBar = 1;
 constexpr int kEpiBar = 2;
-constexpr int kBatch = 2;                     // J postings per thread per load batch
+// J postings per thread per load batch: 3, or 2 when the thread also holds
+// explicit rare-pair records in registers (64 registers a thread)
+template <bool EX>
+constexpr int batch_postings() { return EX ? 2 : 3; }
 constexpr int kUnitRing = 8;                  // unit ids published ahead by the producer
 constexpr int kUnitReaders = 1 + kTW + kEW;   // MMA thread + tail warps + epilogue warps
 static_assert(kSlabCols == 32, "slab accumulator rows are 32 ints (8 swizzled groups)");
@@ -234,7 +237,7 @@ struct MmaArgs {
   int nkc;  // p / 64
 };
 
-template <int STAGES, int CAP, int JW>
+template <int STAGES, int CAP, int JW, bool EX>
 __global__ void __launch_bounds__(kThreads, 1) k_tiles_mma(const TileArgs A, const MmaArgs M) {
   extern __shared__ uint8_t smem_raw[];
   const SmemM S = carve<STAGES, CAP, JW>(smem_raw);
@@ -402,6 +405,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_tiles_mma(const TileArgs A, con
       uint32_t hc[kJSegs + 1], hn[kJSegs + 1];
 #pragma unroll
       for (int m = 0; m <= kJSegs; ++m) hc[m] = (uint32_t)A.hptrJ[kJSegs * U.y + m];
+      constexpr int kBatch = batch_postings<EX>();
       uint2 nxt[kBatch];
       load_batch<kBatch>(A, hc[0], hc[1], ttid, kTT, nxt);
       // explicit rare-feature records: the bounds of the current and the next
@@ -410,7 +414,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_tiles_mma(const TileArgs A, con
       uint32_t ec0 = 0, ec1 = 0, en0 = 0, en1 = 0;
       uint32_t rc = kNoRecord, rn = kNoRecord;
       int rv = 0, rnv = 0;
-      if (A.ex_off) {
+      if (EX) {
         const int64_t t0 = tile_index(I, U.y, A.nbI);
         ec0 = A.ex_off[t0];
         ec1 = A.ex_off[t0 + 1];
@@ -420,7 +424,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_tiles_mma(const TileArgs A, con
         if (J + 1 < U.z) {
 #pragma unroll
           for (int m = 0; m <= kJSegs; ++m) hn[m] = (uint32_t)A.hptrJ[kJSegs * (J + 1) + m];
-          if (A.ex_off) {
+          if (EX) {
             const int64_t t1 = tile_index(I, J + 1, A.nbI);
             en0 = A.ex_off[t1];
             en1 = A.ex_off[t1 + 1];
@@ -436,7 +440,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_tiles_mma(const TileArgs A, con
           // the next slab of this unit: its first batch, in flight from here
           if (q + 1 < kSlabs) load_batch<kBatch>(A, hc[q + 1], hc[q + 2], ttid, kTT, nxt);
           else if (J + 1 < U.z) load_batch<kBatch>(A, hn[0], hn[1], ttid, kTT, nxt);
-          if (q == kSlabs - 2 && A.ex_off && J + 1 < U.z) load_record(A, en0, en1, ttid, rn, rnv);
+          if (EX && q == kSlabs - 2 && J + 1 < U.z) load_record(A, en0, en1, ttid, rn, rnv);
           live = warp_wait(A, &S.aempty[k], (use & 1u) ^ 1u, abort, live);
           int* acc = S.acc + k * kSlabInts;
           const int cofs = q * kSlabCols;
@@ -455,9 +459,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_tiles_mma(const TileArgs A, con
               named_bar(kTailBar, kTT);  // staging rewritten by the next chunk
             }
           }
-          if (live && rc != kNoRecord && (int)((rc & 127u) >> 5) == q)
+          if (EX && live && rc != kNoRecord && (int)((rc & 127u) >> 5) == q)
             atomicAdd(acc + acc_cell<true>((int)(rc >> 7), (int)(rc & 31u), kSlabCols), rv);
-          if (live && ec1 - ec0 > (uint32_t)kTT)
+          if (EX && live && ec1 - ec0 > (uint32_t)kTT)
             tail_explicit<true>(A, ec0 + kTT, ec1, acc, kSlabCols, cofs, kSlabCols, ttid, kTT);
           __syncwarp();
           if (live && lane == 0) mbar_arrive(&S.afull[k]);
@@ -616,9 +620,20 @@ constexpr int kBigStages = 3, kBigCap = 12768;
 
 template <int STAGES, int CAP, int JW>
 cudaError_t set_smem_attr() {
-  return cudaFuncSetAttribute(k_tiles_mma<STAGES, CAP, JW>,
+  cudaError_t e = cudaFuncSetAttribute(k_tiles_mma<STAGES, CAP, JW, false>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)Cfg<STAGES, CAP, JW>::kSmem);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(k_tiles_mma<STAGES, CAP, JW, true>,
                               cudaFuncAttributeMaxDynamicSharedMemorySize,
                               (int)Cfg<STAGES, CAP, JW>::kSmem);
+}
+
+// The kernel of variant (STAGES, CAP, JW), with or without explicit records.
+template <int STAGES, int CAP, int JW>
+cudaError_t launch_variant(const cudaLaunchConfig_t& cfg, const TileArgs& a, const MmaArgs& m) {
+  if (a.ex_off) return cudaLaunchKernelEx(&cfg, k_tiles_mma<STAGES, CAP, JW, true>, a, m);
+  return cudaLaunchKernelEx(&cfg, k_tiles_mma<STAGES, CAP, JW, false>, a, m);
 }
 
 // Opts the kernels into their dynamic shared memory once per device (outside
@@ -661,12 +676,9 @@ cuapss_status launch_tiles_mma(const TileArgs& a, const void* headI16, const voi
   attr[0].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = attr;
   cfg.numAttrs = overlap_prev ? 1 : 0;
-  if (variant == 0)
-    CU_TRY(cudaLaunchKernelEx(&cfg, k_tiles_mma<kWideStages, kWideCap, 2>, a, m));
-  else if (variant == 1)
-    CU_TRY(cudaLaunchKernelEx(&cfg, k_tiles_mma<kSmallStages, kSmallCap, 1>, a, m));
-  else
-    CU_TRY(cudaLaunchKernelEx(&cfg, k_tiles_mma<kBigStages, kBigCap, 1>, a, m));
+  if (variant == 0) CU_TRY((launch_variant<kWideStages, kWideCap, 2>(cfg, a, m)));
+  else if (variant == 1) CU_TRY((launch_variant<kSmallStages, kSmallCap, 1>(cfg, a, m)));
+  else CU_TRY((launch_variant<kBigStages, kBigCap, 1>(cfg, a, m)));
   LAUNCH_CHECK();
   return CUAPSS_OK;
 }
