@@ -555,9 +555,10 @@ def run_selfjoin(args, rank, world, local):
                 "same_pair_set_as_headline": same_pairs(R4),
                 "roofline": tile_roofline(st4, int(st4[-1]["head_width"]), pairs_per_step, x.n,
                                           1, True, x, pk),
-                "note": f"the workload names a {ph}-feature dense head; the library picks "
-                        f"p = {p}, the measured optimum of tensor-core head work (2p flops per "
-                        f"pair) against sparse tail work"}
+                "note": f"the workload names a {ph}-feature dense head; the library's "
+                        f"cost model picks p = {p} and the rare-feature threshold together, "
+                        f"trading tensor-core head work (2p flops per pair) against sparse "
+                        f"tail work"}
             R4.close()
 
         # ---- the plain FP32 hybrid on the same data ----
