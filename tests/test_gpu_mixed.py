@@ -58,6 +58,20 @@ def test_mixed_cross_join(mixed_ctx):
     _check_pairs(mixed_ctx.join(a, b, 0.6), oracle.join(a, b, 0.6))
 
 
+@pytest.mark.parametrize("n", [3000, 3001 + 128, 5000])
+def test_mixed_two_block_mma_tiles(n):
+    # a head as wide as d leaves no tail: the plan is head-bound, so the
+    # tiles are MMAs of N = 256 over two J blocks (and N = 128 for a unit's
+    # last block when its J range has an odd length); self- and cross-join
+    x = synth.generate("plain_20k", n=n + 4000)
+    d64 = (x.d + 63) // 64 * 64
+    a, b = x.rows(0, n), x.rows(n, n + 4000)
+    with cuapss.Context(precision=cuapss.PREC_MIXED, head_width=d64) as c:
+        _check_pairs(c.run(a, 0.6), oracle.apss(a, 0.6))
+        assert c.last_stats["head_width"] == d64
+        _check_pairs(c.join(a, b, 0.6), oracle.join(a, b, 0.6))
+
+
 def test_mixed_matches_fp32_path():
     x = synth.generate("plain_800k", n=30000)
     with cuapss.Context(precision=cuapss.PREC_MIXED) as m, cuapss.Context() as f:
