@@ -67,6 +67,10 @@ constexpr double kExplicitPairSmNs = 7.5;
 // loads J postings two at a time instead of three: 7% slower per tile at
 // equal work (n = 800k, d = 50k: 1,017 against 945 ms with few records).
 constexpr double kExplicitKernelFactor = 1.07;
+// Self-joins of fewer rows skip the rare-feature planning: its statistics
+// kernel and host round trip cost about as much as the pairs could save
+// (measured on 4,096 instances of 64..20,000 rows called one by one).
+constexpr int64_t kRareMinRows = 16384;
 
 struct TileCostModel {
   double head_chunk_ns, tail_posting_ns, overlap_loss;
@@ -262,7 +266,10 @@ cuapss_status join_device(cuapss_ctx* ctx, const DevCsr& a, const DevCsr* b, flo
   // cost their build and their additions.
   std::vector<RareCandidate> rare;
   const int forced_rare = ctx->opts.rare_max_count;
-  if (self && nshards == 1 && ctx->opts.remap && forced_rare >= 0) {
+  // below kRareMinRows rows the pairs cannot pay for the planning's extra
+  // host round trips (unless forced)
+  if (self && nshards == 1 && ctx->opts.remap &&
+      (forced_rare > 0 || (forced_rare == 0 && a.n >= kRareMinRows))) {
     ST_TRY(rare_feature_candidates(counts, d, ws, st, &rare));
     if (forced_rare > 0) {
       std::vector<RareCandidate> keep;

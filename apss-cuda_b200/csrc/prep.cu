@@ -897,6 +897,12 @@ __device__ __forceinline__ bool place_pair(bool valid, uint64_t key, uint32_t vb
   return true;
 }
 
+// Dynamic shared memory of k_rare_place: the range's tile cursors, then for
+// up to kRareProgress postings of the block their sorted position, pair
+// count and progress.
+constexpr size_t kRarePlaceSmem =
+    (size_t)kRareTileChunk * 4 + (size_t)kRareProgress * (4 + 2 + 2);
+
 // The same CTAs place every pair's record at its tile's shared-memory
 // cursor (ex_off holds the tiles' first records). They do so one phase of
 // kRarePhase J blocks at a time, so that the cursors being written at once,
@@ -909,8 +915,11 @@ __global__ void __launch_bounds__(kRareThreads)
                  const uint32_t* __restrict__ inv, const int32_t* __restrict__ cnt,
                  const int64_t* __restrict__ rptr, int64_t n, int rbits, int64_t nb,
                  const uint32_t* __restrict__ ex_off, uint64_t* __restrict__ rec) {
-  __shared__ uint32_t cur[kRareTileChunk];
-  __shared__ uint16_t prog[kRareProgress];
+  extern __shared__ uint8_t place_smem[];
+  uint32_t* cur = reinterpret_cast<uint32_t*>(place_smem);
+  uint32_t* sk = cur + kRareTileChunk;  // sorted position of each posting
+  uint16_t* prog = reinterpret_cast<uint16_t*>(sk + kRareProgress);
+  uint16_t* sc = prog + kRareProgress;  // its pair count (< kMaxRareCount)
   const int64_t I = blockIdx.x;
   const int64_t J0 = max(I, (int64_t)blockIdx.y * kRareTileChunk);
   const int64_t J1 = min(nb, ((int64_t)blockIdx.y + 1) * kRareTileChunk);
@@ -927,6 +936,8 @@ __global__ void __launch_bounds__(kRareThreads)
     for (int64_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
       const uint32_t k = inv[i];
       const int c = cnt[k];
+      sk[i - lo] = k;
+      sc[i - lo] = (uint16_t)c;
       prog[i - lo] = (uint16_t)(J0 == I || c == 0 ? 0 : first_row_at(keys, k, c, rmask,
                                                                         J0 * kBlockRows));
     }
@@ -941,9 +952,15 @@ __global__ void __launch_bounds__(kRareThreads)
       uint32_t k = 0;
       int c = 0, q0 = 0;
       if (i0 + lane < hi) {
-        k = inv[i0 + lane];
-        c = cnt[k];
-        if (c > 0) q0 = keep ? (int)prog[i0 + lane - lo] : first_row_at(keys, k, c, rmask, rlo);
+        if (keep) {  // the headers of every phase after the first come from shared memory
+          k = sk[i0 + lane - lo];
+          c = sc[i0 + lane - lo];
+          q0 = prog[i0 + lane - lo];
+        } else {
+          k = inv[i0 + lane];
+          c = cnt[k];
+          if (c > 0) q0 = first_row_at(keys, k, c, rmask, rlo);
+        }
       }
       const bool live = q0 < c;
       const int64_t ra = live ? (int64_t)(keys[k] & rmask) : 0;
@@ -1054,8 +1071,20 @@ cuapss_status build_explicit_pairs(Side& s, const PrepOptions& o, int64_t* rcoun
   k_rare_tile_counts<<<grid, kRareThreads, 0, st>>>(keys, inv, cnt, rptr, n, rbits, nb, off);
   LAUNCH_CHECK();
   ST_TRY(exclusive_scan<uint32_t>(off, off, ntiles, off + ntiles, ws, t + "ex_scan", st));
-  k_rare_place<<<grid, kRareThreads, 0, st>>>(keys, vs, inv, cnt, rptr, n, rbits, nb, off,
-                                              s.ex_rec);
+  {
+    static std::mutex mu;
+    static uint64_t done = 0;  // attribute set, bit per device
+    int dev = 0;
+    CU_TRY(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lk(mu);
+    if (dev >= 64 || !((done >> dev) & 1ull)) {
+      CU_TRY(cudaFuncSetAttribute(k_rare_place, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)kRarePlaceSmem));
+      if (dev < 64) done |= 1ull << dev;
+    }
+  }
+  k_rare_place<<<grid, kRareThreads, kRarePlaceSmem, st>>>(keys, vs, inv, cnt, rptr, n, rbits,
+                                                          nb, off, s.ex_rec);
   LAUNCH_CHECK();
   return CUAPSS_OK;
 }
