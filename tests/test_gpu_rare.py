@@ -12,7 +12,10 @@ normally chosen with the head width by the cost model; these tests force it
 * 256 rows whose 2,000 shared rare features give one tile about 1,000
   records, more than the mixed kernel holds in registers (the rest are read
   where they are added);
-* the cost model's own choice at 20,000 rows takes explicit pairs."""
+* the cost model's own choice at 40,000 rows takes explicit pairs (below
+  32,768 rows it plans none);
+* 1.1M rows, whose tile rows span more J blocks than one counting CTA
+  covers."""
 import numpy as np
 import pytest
 
@@ -93,12 +96,33 @@ def test_tile_with_many_records(precision, name):
 
 
 def test_model_takes_explicit_pairs():
-    x = synth.generate("mixed_1m", n=20000)
+    x = synth.generate("mixed_1m", n=40000)
     rows = np.random.default_rng(5).choice(x.n, size=200, replace=False)
     wi, wj, ws = oracle.rows(x, 0.7, rows)
     with cuapss.Context(precision=cuapss.PREC_MIXED) as c:
         gi, gj, gs = c.run(x, 0.7, capacity=1 << 20)
         st = c.last_stats
     assert st["explicit_pairs"] > 0 and st["rare_max_count"] >= 16
+    with cuapss.Context(precision=cuapss.PREC_MIXED) as c:
+        c.run(x.rows(0, 20000), 0.7)
+        assert c.last_stats["explicit_pairs"] == 0  # too small to plan
+    sel = np.isin(gi, rows) | np.isin(gj, rows)
+    _check((gi[sel], gj[sel], gs[sel]), (wi, wj, ws))
+
+
+def test_tile_rows_past_one_counting_range():
+    # 1.1M rows: 8,594 row blocks, more than the 8,192 J blocks one counting
+    # / placement CTA covers, so the tile rows are split over two CTAs (the
+    # second starts above the diagonal and finds each posting's first pair
+    # in its range by binary search)
+    x = synth.generate("mixed_1m", n=1_100_000)
+    rows = np.random.default_rng(8).choice(x.n, size=64, replace=False)
+    rows = np.concatenate([rows, [x.n - 1, 0, 8192 * 128 + 5]]).astype(np.int32)
+    wi, wj, ws = oracle.rows(x, 0.5, rows)
+    assert len(wi) > 500
+    with cuapss.Context(precision=cuapss.PREC_MIXED, head_width=1024, rare_max_count=128) as c:
+        gi, gj, gs = c.run(x, 0.5, capacity=1 << 25)
+        st = c.last_stats
+    assert st["rare_max_count"] == 128 and st["explicit_pairs"] > 0
     sel = np.isin(gi, rows) | np.isin(gj, rows)
     _check((gi[sel], gj[sel], gs[sel]), (wi, wj, ws))
