@@ -79,6 +79,7 @@ struct TileCostModel {
 constexpr TileCostModel kProbedTail{388.0, 1.6, 0.06};
 constexpr TileCostModel kRarePaired{340.0, 1.84, 0.3};
 constexpr int kMaxModelHead = 8192;
+constexpr double kUnitCostCap = 512.0;  // unit cost cap (tile weights, 1 + tail / mean)
 
 namespace {
 
@@ -382,8 +383,12 @@ cuapss_status join_device(cuapss_ctx* ctx, const DevCsr& a, const DevCsr* b, flo
     double total = 0.0;
     for (int I = shard; I < SA.nb; I += nshards) total += weight(I) * (SJ->nb - (self ? I : 0));
     // about 64 units per CTA: the CTAs take them dynamically, so the last
-    // ones to finish wait at most a short unit
-    const double target = std::max(1.0, total / (grid_max * 64.0));
+    // ones to finish wait at most a short unit. A unit costs at most about
+    // kUnitCostCap (about 256 tiles of mean weight), so that the J windows
+    // of the units running at one time stay within L2: the J operands of a
+    // 3,200-tile unit (n = 1M, 64 units per CTA) span 0.8 GB, and the tile
+    // kernel then read 4.1 TB from DRAM per launch.
+    const double target = std::max(1.0, std::min(total / (grid_max * 64.0), kUnitCostCap));
     for (int I = shard; I < SA.nb; I += nshards) {
       const int jb = self ? I : 0, je = SJ->nb;
       const int chunk = (int)std::max(1.0, std::floor(target / weight(I)));
