@@ -321,8 +321,9 @@ def tile_roofline(stats, p, pairs, n, world, prec_mixed, x, peaks_):
         return {"bound": "tensor", "achieved": achieved, "peak": bf16_sus, "unit": "TFLOP/s",
                 "frac": achieved / bf16_sus,
                 "traffic": traffic,
-                "traffic_source": "ncu launch list at 200,000 rows of this shape, scaled by "
-                                  "tiles x p / 64 (profiles/launches_mixed1m_n200k_dram.md)",
+                "traffic_source": "one-pass ncu capture of the full-size n = d = 1M launch, "
+                                  "scaled by tiles x p / 64 "
+                                  "(profiles/k_tiles_mma_mixed1m_n1m_dram.md)",
                 "peak_source": f"{src} (sustained BF16: the kernel runs for about a second "
                                f"inside a multi-second step)",
                 "frac_of_burst": achieved / bf16,
@@ -340,12 +341,10 @@ def tile_roofline(stats, p, pairs, n, world, prec_mixed, x, peaks_):
 
 
 # DRAM bytes (read + write) of k_tiles_mma per 128 x 128 tile and 64 head
-# features, from the ncu launch list of the n = d = 1M workload's shape at
-# 200,000 rows (10.39 GB over 1,222,266 tiles at p = 960; the full-size launch
-# is too large to capture with several metrics). Scaled by tiles x p / 64; at
-# full size the head block is a larger multiple of the L2, so the true figure
-# may be higher.
-TILE_TRAFFIC_PER_CHUNK = 10.39e9 / 1_222_266 / 15
+# features, from a one-pass ncu capture of the full-size n = d = 1M launch
+# (263.2 GB over 30,525,391 tiles at p = 1,024). Scaled by tiles x p / 64 for
+# other sizes and head widths.
+TILE_TRAFFIC_PER_CHUNK = 263.2e9 / 30_525_391 / 16
 
 
 def dry_shards(args, rank, world):
