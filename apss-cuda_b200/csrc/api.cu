@@ -261,7 +261,8 @@ cuapss_status join_device(cuapss_ctx* ctx, const DevCsr& a, const DevCsr* b, flo
   ST_TRY(feature_perm(counts, d, a.n + (self ? 0 : bb.n), ctx->opts.remap, perm, ws, st));
   const int precision = ctx->opts.precision;
   // Tail features that occur in at most a few rows are paired explicitly
-  // (self-joins on one shard): probing their postings in every tile is
+  // (self-joins; a shard builds the pairs of its own tile rows): probing
+  // their postings in every tile is
   // almost all misses. They are the highest ranks only under the frequency
   // remap. The threshold and the head width are chosen together: the head
   // is sized against the tail that is still probed, each threshold's pairs
@@ -270,7 +271,7 @@ cuapss_status join_device(cuapss_ctx* ctx, const DevCsr& a, const DevCsr* b, flo
   const int forced_rare = ctx->opts.rare_max_count;
   // below kRareMinRows rows the pairs cannot pay for the planning's extra
   // host round trips (unless forced)
-  if (self && nshards == 1 && ctx->opts.remap &&
+  if (self && ctx->opts.remap &&
       (forced_rare > 0 || (forced_rare == 0 && a.n >= kRareMinRows))) {
     ST_TRY(rare_feature_candidates(counts, d, ws, st, &rare));
     if (forced_rare > 0) {
@@ -314,6 +315,8 @@ cuapss_status join_device(cuapss_ctx* ctx, const DevCsr& a, const DevCsr* b, flo
     // the head keeps its p ranks in any case
     po.rare_from = std::max<int64_t>(plan.rare.rank, p);
     po.rare_max_count = plan.rare.max_count;
+    po.rare_shard = shard;
+    po.rare_nshards = nshards;
   }
   const bool head_bound = mixed && head_bound_plan(p, n_all, nnz_all, prefix, plan.rare);
   Side SA, SB;

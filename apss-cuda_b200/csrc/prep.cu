@@ -830,7 +830,8 @@ constexpr int kRareProgress = 8192;   // postings per row block with progress in
 __global__ void __launch_bounds__(kRareThreads)
     k_rare_tile_counts(const uint64_t* __restrict__ keys, const uint32_t* __restrict__ inv,
                        const int32_t* __restrict__ cnt, const int64_t* __restrict__ rptr,
-                       int64_t n, int rbits, int64_t nb, uint32_t* __restrict__ ex_off) {
+                       int64_t n, int rbits, int64_t nb, int shard, int nshards,
+                       uint32_t* __restrict__ ex_off) {
   __shared__ uint32_t sm[kRareTileChunk];
   const int64_t I = blockIdx.x;
   const int64_t J0 = max(I, (int64_t)blockIdx.y * kRareTileChunk);
@@ -838,6 +839,10 @@ __global__ void __launch_bounds__(kRareThreads)
   if (J0 >= J1) return;  // the whole CTA: a range below the diagonal
   const int nj = (int)(J1 - J0);
   const int64_t tbase = tile_index(I, J0, nb);
+  if (I % nshards != shard) {  // another shard's tile row: no records here
+    for (int j = threadIdx.x; j < nj; j += blockDim.x) ex_off[tbase + j] = 0u;
+    return;
+  }
   for (int j = threadIdx.x; j < nj; j += blockDim.x) sm[j] = 0u;
   __syncthreads();
   const uint64_t rmask = (1ull << rbits) - 1ull;
@@ -913,9 +918,10 @@ constexpr size_t kRarePlaceSmem =
 __global__ void __launch_bounds__(kRareThreads)
     k_rare_place(const uint64_t* __restrict__ keys, const uint32_t* __restrict__ vs,
                  const uint32_t* __restrict__ inv, const int32_t* __restrict__ cnt,
-                 const int64_t* __restrict__ rptr, int64_t n, int rbits, int64_t nb,
-                 const uint32_t* __restrict__ ex_off, uint64_t* __restrict__ rec) {
+                 const int64_t* __restrict__ rptr, int64_t n, int rbits, int64_t nb, int shard,
+                 int nshards, const uint32_t* __restrict__ ex_off, uint64_t* __restrict__ rec) {
   extern __shared__ uint8_t place_smem[];
+  if ((int64_t)blockIdx.x % nshards != shard) return;  // another shard's tile row
   uint32_t* cur = reinterpret_cast<uint32_t*>(place_smem);
   uint32_t* sk = cur + kRareTileChunk;  // sorted position of each posting
   uint16_t* prog = reinterpret_cast<uint16_t*>(sk + kRareProgress);
@@ -1060,17 +1066,24 @@ cuapss_status build_explicit_pairs(Side& s, const PrepOptions& o, int64_t* rcoun
   unsigned long long P = 0;
   CU_TRY(cudaMemcpyAsync(&P, total, sizeof(P), cudaMemcpyDeviceToHost, st));
   CU_TRY(cudaStreamSynchronize(st));
+  // all of the self-join's pairs; a shard keeps those of its tile rows
   if (P >= (unsigned long long)UINT32_MAX - 1) return CUAPSS_EINVAL;
-  s.n_explicit = (int64_t)P;
+  s.n_explicit = 0;
   if (P == 0) {
     CU_TRY(cudaMemsetAsync(off, 0, sizeof(uint32_t) * (ntiles + 1), st));
     return CUAPSS_OK;
   }
-  ST_TRY(ws.get(t + "ex_rec", (size_t)P, &s.ex_rec));
   const dim3 grid((unsigned)nb, (unsigned)((nb + kRareTileChunk - 1) / kRareTileChunk));
-  k_rare_tile_counts<<<grid, kRareThreads, 0, st>>>(keys, inv, cnt, rptr, n, rbits, nb, off);
+  k_rare_tile_counts<<<grid, kRareThreads, 0, st>>>(keys, inv, cnt, rptr, n, rbits, nb,
+                                                    o.rare_shard, o.rare_nshards, off);
   LAUNCH_CHECK();
   ST_TRY(exclusive_scan<uint32_t>(off, off, ntiles, off + ntiles, ws, t + "ex_scan", st));
+  uint32_t kept = 0;
+  CU_TRY(cudaMemcpyAsync(&kept, off + ntiles, sizeof(kept), cudaMemcpyDeviceToHost, st));
+  CU_TRY(cudaStreamSynchronize(st));
+  s.n_explicit = kept;
+  if (kept == 0) return CUAPSS_OK;
+  ST_TRY(ws.get(t + "ex_rec", (size_t)kept, &s.ex_rec));
   {
     static std::mutex mu;
     static uint64_t done = 0;  // attribute set, bit per device
@@ -1084,7 +1097,8 @@ cuapss_status build_explicit_pairs(Side& s, const PrepOptions& o, int64_t* rcoun
     }
   }
   k_rare_place<<<grid, kRareThreads, kRarePlaceSmem, st>>>(keys, vs, inv, cnt, rptr, n, rbits,
-                                                          nb, off, s.ex_rec);
+                                                          nb, o.rare_shard, o.rare_nshards, off,
+                                                          s.ex_rec);
   LAUNCH_CHECK();
   return CUAPSS_OK;
 }

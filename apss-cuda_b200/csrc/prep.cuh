@@ -20,6 +20,10 @@ struct PrepOptions {
   // rare_max_count rows) are paired explicitly instead of probed; 0: off.
   int64_t rare_from = 0;
   int rare_max_count = 0;
+  // Row-block shard of a self-join: only the explicit pairs of the tiles
+  // (I, J) with I % rare_nshards == rare_shard are built.
+  int rare_shard = 0;
+  int rare_nshards = 1;
 };
 
 // Validates a device CSR. counts (device, d entries, may be null) are

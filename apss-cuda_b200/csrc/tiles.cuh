@@ -38,7 +38,7 @@ struct TileArgs {
   const int64_t* hptrJ;     // postings of each kJSegRows-row segment of J
   const uint2* bilJ_rec;    // packed postings {feature << 8 | row, value bits}
   // explicit pairs of rare features (self-joins; null: none): records of
-  // tile (I, J) at [ex_off[t], ex_off[t + 1]), t = tri_tile(I, J, nbI):
+  // tile (I, J) at [ex_off[t], ex_off[t + 1]), t = tile_index(I, J, nbI):
   // {fixed-point product << 32 | row in I block << 7 | column in J block}
   const uint32_t* ex_off;
   const uint64_t* ex_rec;

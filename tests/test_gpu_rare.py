@@ -15,7 +15,8 @@ normally chosen with the head width by the cost model; these tests force it
 * the cost model's own choice at 40,000 rows takes explicit pairs (below
   32,768 rows it plans none);
 * 1.1M rows, whose tile rows span more J blocks than one counting CTA
-  covers."""
+  covers;
+* row-block shards, each building the pairs of its own tile rows."""
 import numpy as np
 import pytest
 
@@ -126,3 +127,26 @@ def test_tile_rows_past_one_counting_range():
     assert st["rare_max_count"] == 128 and st["explicit_pairs"] > 0
     sel = np.isin(gi, rows) | np.isin(gj, rows)
     _check((gi[sel], gj[sel], gs[sel]), (wi, wj, ws))
+
+
+@pytest.mark.parametrize("precision,name", PRECISIONS, ids=[n for _, n in PRECISIONS])
+def test_shards_with_explicit_pairs(zipf8k, precision, name):
+    # each row-block shard builds the explicit pairs of its own tile rows;
+    # the shards' union equals the whole join and the oracle, bit for bit
+    x, want = zipf8k
+    with cuapss.Context(precision=precision, rare_max_count=256) as c:
+        full = c.run(x, 0.5, capacity=1 << 20)
+        whole = c.last_stats["explicit_pairs"]
+        _check(full, want)
+        for nshards in (2, 3):
+            parts, kept = [], 0
+            for s in range(nshards):
+                parts.append(c.run_shard(x, 0.5, s, nshards, capacity=1 << 20))
+                assert c.last_stats["rare_max_count"] == 256
+                kept += c.last_stats["explicit_pairs"]
+                assert np.all((parts[-1][0] // 128) % nshards == s)
+            assert kept == whole  # every pair in exactly one shard
+            key = np.concatenate([p[0].astype(np.int64) * x.n + p[1] for p in parts])
+            order = np.argsort(key)
+            assert np.array_equal(key[order], full[0].astype(np.int64) * x.n + full[1])
+            assert np.array_equal(np.concatenate([p[2] for p in parts])[order], full[2])
