@@ -356,11 +356,16 @@ def dry_shards(args, rank, world):
     import torch.distributed as dist
 
     import cuapss
-    dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=60))
+    single = world == 1 and "RANK" not in os.environ  # one rank, no launcher
+    if not single:
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=60))
     n = args.n or 1_000_000
     mine = [int(b) for b in cuapss.shard_blocks(n, rank, world)]
     objs = [None] * world
-    dist.all_gather_object(objs, mine)
+    if single:
+        objs[0] = mine
+    else:
+        dist.all_gather_object(objs, mine)
     if rank == 0:
         nb = (n + 127) // 128
         allb = sorted(b for o in objs for b in o)
@@ -369,8 +374,9 @@ def dry_shards(args, rank, world):
                           "n": n, "blocks": nb, "shard_blocks": [len(o) for o in objs],
                           "shard_tiles": tiles, "partition_ok": allb == list(range(nb)),
                           "parallelism": f"row-block shards x{world}"}))
-    dist.barrier()
-    dist.destroy_process_group()
+    if not single:
+        dist.barrier()
+        dist.destroy_process_group()
 
 
 def run_selfjoin(args, rank, world, local):
