@@ -12,6 +12,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <functional>
 #include <cmath>
 #include <cstring>
 #include <mutex>
@@ -184,6 +185,59 @@ TilePlan plan_tiles(int precision, int64_t n, int64_t d, int64_t nnz,
     }
   }
   return plan;
+}
+
+namespace {
+
+// Candidates of rare_feature_candidates from host counts (same thresholds).
+void host_rare_candidates(const int32_t* counts, int64_t d, std::vector<RareCandidate>* out) {
+  out->clear();
+  for (int C = kMaxRareCount; C >= 16; C >>= 1) {
+    RareCandidate c;
+    c.max_count = C;
+    for (int64_t f = 0; f < d; ++f) {
+      const int64_t k = counts[f];
+      if (k > C) {
+        ++c.rank;
+      } else {
+        c.pairs += k * (k - 1) / 2;
+        c.postings += k;
+      }
+    }
+    if (c.postings > 0) out->push_back(c);
+  }
+}
+
+}  // namespace
+
+extern "C" cuapss_status cuapss_plan_self_join(int32_t precision, int64_t n, int64_t d,
+                                               const int32_t* counts, int64_t max_pairs,
+                                               int32_t* head_width, int32_t* rare_max_count,
+                                               int64_t* explicit_pairs) {
+  if (n < 0 || d < 1 || d > INT32_MAX || !counts || !head_width) return CUAPSS_EINVAL;
+  if (precision != CUAPSS_PREC_FP32 && precision != CUAPSS_PREC_MIXED) return CUAPSS_EINVAL;
+  for (int64_t f = 0; f < d; ++f)
+    if (counts[f] < 0 || counts[f] > n) return CUAPSS_EINVAL;
+  // the posting counts of the most frequent features, as rank_count_prefix
+  std::vector<int32_t> sorted(counts, counts + d);
+  const int64_t top = std::min<int64_t>(d, kMaxModelHead);
+  std::partial_sort(sorted.begin(), sorted.begin() + top, sorted.end(), std::greater<int32_t>());
+  std::vector<int64_t> prefix((size_t)top + 1, 0);
+  for (int64_t k = 0; k < top; ++k) prefix[(size_t)k + 1] = prefix[(size_t)k] + sorted[(size_t)k];
+  int64_t nnz = 0;
+  for (int64_t f = 0; f < d; ++f) nnz += counts[f];
+  std::vector<RareCandidate> rare;
+  if (n >= kRareMinRows) host_rare_candidates(counts, d, &rare);
+  const int64_t bound = max_pairs > 0 ? std::min(max_pairs, kMaxExplicitPairs) : kMaxExplicitPairs;
+  const TilePlan plan = plan_tiles(precision, n, d, nnz, prefix, rare, bound, 0);
+  const bool mixed = precision == CUAPSS_PREC_MIXED;
+  const int pq = mixed ? 64 : 32;  // as the self-join rounds it
+  int p = (int)std::min<int64_t>(((int64_t)plan.p + pq - 1) / pq * pq, ((d + pq - 1) / pq) * pq);
+  if (mixed && p < 64) p = 64;
+  *head_width = p;
+  if (rare_max_count) *rare_max_count = plan.rare.max_count;
+  if (explicit_pairs) *explicit_pairs = plan.rare.max_count > 0 ? plan.rare.pairs : 0;
+  return CUAPSS_OK;
 }
 
 cuapss_status stage_csr(cuapss_ctx* ctx, const cuapss_csr* x, const std::string& tag,

@@ -165,6 +165,11 @@ def lib():
         L.cuapss_shard_blocks.argtypes = [ctypes.c_int64, ctypes.c_int32, ctypes.c_int32, _P,
                                           ctypes.c_int64]
         L.cuapss_shard_blocks.restype = ctypes.c_int32
+        L.cuapss_plan_self_join.argtypes = [ctypes.c_int32, ctypes.c_int64, ctypes.c_int64, _P,
+                                            ctypes.c_int64, ctypes.POINTER(ctypes.c_int32),
+                                            ctypes.POINTER(ctypes.c_int32),
+                                            ctypes.POINTER(ctypes.c_int64)]
+        L.cuapss_plan_self_join.restype = ctypes.c_int
         L.cuapss_index_create.argtypes = [_P, ctypes.POINTER(CsrDesc), ctypes.POINTER(_P)]
         L.cuapss_index_create.restype = ctypes.c_int
         L.cuapss_index_append.argtypes = [_P, _P, ctypes.POINTER(CsrDesc)]
@@ -537,6 +542,25 @@ class Server:
             self.close()
         except Exception:
             pass
+
+
+def plan_self_join(x, precision: int = PREC_MIXED, max_pairs: int = 0) -> dict:
+    """The plan cuapss_run makes for a self-join of x (a Csr, or a pair
+    (posting counts per feature, n rows)), computed on the host: head width,
+    rare-feature threshold (0: none) and the explicit pairs it implies."""
+    if isinstance(x, tuple):
+        counts, n = x
+        counts = np.ascontiguousarray(counts, dtype=np.int32)
+    else:
+        counts = np.bincount(x.col, minlength=x.d).astype(np.int32)
+        n = x.n
+    p = ctypes.c_int32()
+    c = ctypes.c_int32()
+    pairs = ctypes.c_int64()
+    _check(lib().cuapss_plan_self_join(int(precision), int(n), len(counts), counts.ctypes.data,
+                                       int(max_pairs), ctypes.byref(p), ctypes.byref(c),
+                                       ctypes.byref(pairs)), "cuapss_plan_self_join")
+    return {"head_width": p.value, "rare_max_count": c.value, "explicit_pairs": pairs.value}
 
 
 def shard_blocks(n: int, shard: int, nshards: int) -> np.ndarray:

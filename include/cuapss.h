@@ -314,6 +314,18 @@ cuapss_status cuapss_build_index(cuapss_ctx* ctx, const cuapss_csr* x,
                                  float* idx_val, int64_t capacity,
                                  int64_t* tail_nnz);
 
+/* The plan cuapss_run makes for a self-join (default options, one shard),
+ * from the posting counts alone, on the host, with no device: counts[f] =
+ * the number of rows that contain feature f (d entries), n rows. Writes the
+ * head width p, the rare-feature threshold C (0: none) and the number of
+ * explicit pairs C implies (before the head's features are taken out).
+ * max_pairs bounds the explicit pairs (<= 0: the library's bound; the run
+ * also bounds them by free device memory). No reference counterpart. */
+cuapss_status cuapss_plan_self_join(int32_t precision, int64_t n, int64_t d,
+                                    const int32_t* counts, int64_t max_pairs,
+                                    int32_t* head_width, int32_t* rare_max_count,
+                                    int64_t* explicit_pairs);
+
 /* Frequency-ordered feature remap: perm[f] = rank of feature f when features
  * are sorted by (posting count descending, id ascending); counts[f] = the
  * posting count. Device pointers if x->on_device. (No counterpart in the

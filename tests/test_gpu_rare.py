@@ -104,6 +104,11 @@ def test_model_takes_explicit_pairs():
         gi, gj, gs = c.run(x, 0.7, capacity=1 << 20)
         st = c.last_stats
     assert st["explicit_pairs"] > 0 and st["rare_max_count"] >= 16
+    # the host planner makes the same choice from the posting counts
+    plan = cuapss.plan_self_join(x)
+    assert plan["head_width"] == st["head_width"]
+    assert plan["rare_max_count"] == st["rare_max_count"]
+    assert 0 < st["explicit_pairs"] <= plan["explicit_pairs"]
     with cuapss.Context(precision=cuapss.PREC_MIXED) as c:
         c.run(x.rows(0, 20000), 0.7)
         assert c.last_stats["explicit_pairs"] == 0  # too small to plan
