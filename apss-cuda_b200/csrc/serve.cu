@@ -16,9 +16,12 @@
 // per segment writes candidates into that segment's region; the finalize of
 // each segment maps its rows to index rows; one sort orders the union.
 //
-// Concurrency. The segment list is swapped under a mutex; a query copies the
+// Concurrency. The segment list is changed under a mutex; a query copies the
 // list (shared pointers) when it starts and holds it until it returns, so an
-// append or merge never frees a segment a running query reads.
+// append or merge never frees a segment a running query reads. An append
+// builds and publishes its segment (index_append_segment); merges are
+// separate steps (index_merge_step) that replace two adjacent segments by
+// their union, so the request server runs them on a thread of its own.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -151,6 +154,7 @@ struct cuapss_index {
   int32_t* perm = nullptr;
   std::mutex mu;        // guards segs, rows, nrm
   std::mutex append_mu;  // one append at a time
+  std::mutex merge_mu;   // one merge at a time
   cuapss::SegList segs;
   int64_t rows = 0;
   double nrm = 0.0;
@@ -311,8 +315,9 @@ extern "C" cuapss_status cuapss_index_create(cuapss_ctx* ctx, const cuapss_csr* 
   return CUAPSS_OK;
 }
 
-extern "C" cuapss_status cuapss_index_append(cuapss_ctx* ctx, cuapss_index* idx,
-                                             const cuapss_csr* x) {
+namespace cuapss {
+
+cuapss_status index_append_segment(cuapss_ctx* ctx, cuapss_index* idx, const cuapss_csr* x) {
   if (!ctx || !idx || !x) return CUAPSS_EINVAL;
   if (ctx->device != idx->device || x->d != idx->d) return CUAPSS_EINVAL;
   if (x->n == 0) return CUAPSS_OK;
@@ -323,39 +328,64 @@ extern "C" cuapss_status cuapss_index_append(cuapss_ctx* ctx, cuapss_index* idx,
   double nrm = 1.0;
   ST_TRY(check_rows(ctx, idx, a, nullptr, &nrm, "AP"));
   if (nrm >= 1.37) return CUAPSS_EINVAL;
-  SegList segs;
   int64_t rows = 0;
   {
     std::lock_guard<std::mutex> lk(idx->mu);
-    segs = idx->segs;
     rows = idx->rows;
   }
   std::shared_ptr<Segment> seg;
   ST_TRY(build_segment(ctx, idx, a, rows, nrm, &seg));
-  segs.push_back(seg);
-  // merge trailing segments of similar size (the newer at least half the
-  // older), and the last two whenever there are too many
-  while (segs.size() >= 2) {
-    const Segment& A = *segs[segs.size() - 2];
-    const Segment& B = *segs[segs.size() - 1];
-    if (!(2 * B.n >= A.n || segs.size() > kMaxSegments)) break;
-    DevCsr m;
-    ST_TRY(concat_segments(ctx, A, B, &m));
-    m.d = idx->d;
-    std::shared_ptr<Segment> merged;
-    ST_TRY(build_segment(ctx, idx, m, A.row0, std::max(A.nrm, B.nrm), &merged));
-    segs.pop_back();
-    segs.pop_back();
-    segs.push_back(merged);
-  }
   // the build temporaries stay in ctx's grow-only workspace: freeing them
   // here would synchronize the device under running queries
+  std::lock_guard<std::mutex> lk(idx->mu);
+  idx->segs.push_back(seg);
+  idx->rows = rows + a.n;
+  idx->nrm = std::max(idx->nrm, nrm);
+  return CUAPSS_OK;
+}
+
+cuapss_status index_merge_step(cuapss_ctx* ctx, cuapss_index* idx, bool* merged) {
+  *merged = false;
+  if (!ctx || !idx || ctx->device != idx->device) return CUAPSS_EINVAL;
+  CU_TRY(cudaSetDevice(ctx->device));
+  std::lock_guard<std::mutex> mlk(idx->merge_mu);  // one merge at a time
+  std::shared_ptr<const Segment> A, B;
   {
+    // merge the trailing segments when they are of similar size (the newer
+    // at least half the older), and the last two whenever there are too many
     std::lock_guard<std::mutex> lk(idx->mu);
-    idx->segs = segs;
-    idx->rows = rows + a.n;
-    idx->nrm = std::max(idx->nrm, nrm);
+    const SegList& segs = idx->segs;
+    if (segs.size() < 2) return CUAPSS_OK;
+    A = segs[segs.size() - 2];
+    B = segs[segs.size() - 1];
+    if (!(2 * B->n >= A->n || segs.size() > kMaxSegments)) return CUAPSS_OK;
   }
+  DevCsr m;
+  ST_TRY(concat_segments(ctx, *A, *B, &m));
+  m.d = idx->d;
+  std::shared_ptr<Segment> ab;
+  ST_TRY(build_segment(ctx, idx, m, A->row0, std::max(A->nrm, B->nrm), &ab));
+  std::lock_guard<std::mutex> lk(idx->mu);
+  // appends may have added segments behind B meanwhile; only merges remove
+  // segments, so A and B are still adjacent
+  SegList& segs = idx->segs;
+  for (size_t k = 0; k + 1 < segs.size(); ++k) {
+    if (segs[k] == A && segs[k + 1] == B) {
+      segs[k] = ab;
+      segs.erase(segs.begin() + (std::ptrdiff_t)(k + 1));
+      *merged = true;
+      break;
+    }
+  }
+  return CUAPSS_OK;
+}
+
+}  // namespace cuapss
+
+extern "C" cuapss_status cuapss_index_append(cuapss_ctx* ctx, cuapss_index* idx,
+                                             const cuapss_csr* x) {
+  ST_TRY(cuapss::index_append_segment(ctx, idx, x));
+  for (bool merged = true; merged;) ST_TRY(cuapss::index_merge_step(ctx, idx, &merged));
   return CUAPSS_OK;
 }
 

@@ -33,9 +33,12 @@
 // Streams. Each lane's context runs on a stream of the device's lowest
 // (default) priority; appends run on one separate context whose stream has
 // the highest priority: the queries queued behind an append wait for it, so
-// the block scheduler starts an append's or a merge's CTAs ahead of pending
-// query CTAs. (The other way round, appends starved behind the lanes'
-// persistent tile kernels: p99 of the mixed workload 560 ms against 240 ms.)
+// the block scheduler starts an append's CTAs ahead of pending query CTAs.
+// (The other way round, appends starved behind the lanes' persistent tile
+// kernels: p99 of the mixed workload 560 ms against 240 ms.) An append only
+// builds its rows' segment; the segment merges it calls for run on a thread
+// of their own with a third context at the lanes' priority, so no lane and
+// no queued query waits for a merge.
 //
 // Appends are taken in submission order by one lane at a time, when they
 // are the oldest queued item; queries queued behind an append wait until
@@ -109,11 +112,14 @@ struct cuapss_server {
   cuapss_server_opts opts{};
   int head_width = 0;
   std::vector<cuapss_ctx*> lanes;
-  cuapss_ctx* append_ctx = nullptr;      // appends and merges, high-priority stream
+  cuapss_ctx* append_ctx = nullptr;      // appends, high-priority stream
+  cuapss_ctx* merge_ctx = nullptr;       // segment merges, the lanes' priority
+  std::thread merger;                    // runs the merges the appends call for
   std::vector<cudaStream_t> streams;     // created here, destroyed after the contexts
   std::vector<std::thread> threads;
   std::mutex mu;
-  std::condition_variable cv_work, cv_done;
+  std::condition_variable cv_work, cv_done, cv_merge;
+  bool merge_due = false;
   std::deque<ReqPtr> queue;
   std::unordered_map<uint64_t, ReqPtr> reqs;
   uint64_t next_id = 1;
@@ -197,10 +203,14 @@ void finish_item(Request& r, cuapss_status st, std::vector<int32_t>&& oi, std::v
 
 void run_append(cuapss_server* s, cuapss_ctx* ctx, const ReqPtr& r) {
   cuapss_csr x{r->n, r->d, (int64_t)r->col.size(), r->rp.data(), r->col.data(), r->val.data(), 0};
-  const cuapss_status st = cuapss_index_append(ctx, s->idx, &x);
+  // the new rows' segment only: its merges run on the merge thread, so the
+  // lane (and the queries queued behind the append) wait for no merge
+  const cuapss_status st = cuapss::index_append_segment(ctx, s->idx, &x);
   int64_t rows = 0;
   cuapss_index_info(s->idx, &rows, nullptr, nullptr, nullptr);
   std::lock_guard<std::mutex> lk(s->mu);
+  s->merge_due = true;
+  s->cv_merge.notify_one();
   r->status = st;
   r->index_rows = rows;
   r->done = Clock::now();
@@ -209,6 +219,23 @@ void run_append(cuapss_server* s, cuapss_ctx* ctx, const ReqPtr& r) {
   r->rp.clear();
   r->col.clear();
   r->val.clear();
+}
+
+// The merge thread: after each append, the merges of the index's trailing
+// segments that the size policy calls for, one at a time, on its own
+// context. A merge that fails leaves the segments as they were (the index
+// stays valid, with more segments).
+void merge_loop(cuapss_server* s) {
+  std::unique_lock<std::mutex> lk(s->mu);
+  while (true) {
+    s->cv_merge.wait(lk, [s] { return s->merge_due || s->stop; });
+    if (s->stop) break;
+    s->merge_due = false;
+    lk.unlock();
+    for (bool merged = true; merged;)
+      if (cuapss::index_merge_step(s->merge_ctx, s->idx, &merged) != CUAPSS_OK) break;
+    lk.lock();
+  }
 }
 
 void run_batch(cuapss_server* s, cuapss_ctx* ctx, std::vector<ReqPtr>& batch, int64_t batch_id,
@@ -448,14 +475,16 @@ cuapss_status cuapss_server_create(cuapss_server** out, cuapss_index* idx, int d
   auto undo = [&s]() {
     for (auto* x : s->lanes) cuapss_destroy(x);
     if (s->append_ctx) cuapss_destroy(s->append_ctx);
+    if (s->merge_ctx) cuapss_destroy(s->merge_ctx);
     for (auto q : s->streams) cudaStreamDestroy(q);
   };
   int least = 0, greatest = 0;
   if (cudaSetDevice(device) != cudaSuccess ||
       cudaDeviceGetStreamPriorityRange(&least, &greatest) != cudaSuccess)
     return CUAPSS_ECUDA;
-  for (int l = 0; l <= opts.lanes; ++l) {  // the lanes, then the append context
-    const bool append = l == opts.lanes;
+  // the lanes, then the append context, then the merge context
+  for (int l = 0; l <= opts.lanes + 1; ++l) {
+    const bool append = l == opts.lanes, merge = l == opts.lanes + 1;
     cudaStream_t q = nullptr;
     if (cudaStreamCreateWithPriority(&q, cudaStreamNonBlocking, append ? greatest : least) !=
         cudaSuccess) {
@@ -474,9 +503,11 @@ cuapss_status cuapss_server_create(cuapss_server** out, cuapss_index* idx, int d
       return st;
     }
     if (append) s->append_ctx = c;
+    else if (merge) s->merge_ctx = c;
     else s->lanes.push_back(c);
   }
   for (int l = 0; l < opts.lanes; ++l) s->threads.emplace_back(lane_loop, s.get(), l);
+  s->merger = std::thread(merge_loop, s.get());
   *out = s.release();
   return CUAPSS_OK;
 }
@@ -552,9 +583,12 @@ cuapss_status cuapss_server_destroy(cuapss_server* s) {
     s->stop = true;
   }
   s->cv_work.notify_all();
+  s->cv_merge.notify_all();
   for (auto& th : s->threads) th.join();
+  if (s->merger.joinable()) s->merger.join();
   for (auto* c : s->lanes) cuapss_destroy(c);
   if (s->append_ctx) cuapss_destroy(s->append_ctx);
+  if (s->merge_ctx) cuapss_destroy(s->merge_ctx);
   for (auto q : s->streams) cudaStreamDestroy(q);
   delete s;
   return CUAPSS_OK;
